@@ -1,0 +1,171 @@
+/* uq_lbm.h - C ABI of the B200 D2Q13 thermal lattice-Boltzmann step.
+ *
+ * Drop-in boundary for the reference solver's step API, the C++ class
+ * cpuLBM (CODE/C++/VS2010/simLB/simLB/cpuLBM.h:16-175) and the PyOpenCL
+ * ClassLBM.runSimStep (CODE/Python/simLB/LBM.py:571-594).  Plain C types
+ * only; every entry point returns an lbm_status and never throws.
+ *
+ * Layout at the boundary is the reference's: per-node arrays are indexed
+ * [x*Ny + y] (macros.h:8-14) and distributions [(x*Ny + y)*13 + i]
+ * (macros.h:9-10).  Inside the library the state is structure-of-arrays on
+ * the GPU; the conversion happens in lbm_get_* / lbm_set_*.
+ *
+ * Threading: a handle is not thread-safe; each handle owns one CUDA stream.
+ * There is no CPU fallback: without a usable CUDA device lbm_create fails
+ * with LBM_ERR_CUDA.
+ */
+#ifndef UQ_LBM_H_
+#define UQ_LBM_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define LBM_API __attribute__((visibility("default")))
+#else
+#define LBM_API
+#endif
+
+typedef enum lbm_status {
+    LBM_OK = 0,
+    /* an equilibrium mass check failed: the reference's hasFailed
+     * (cpuLBM.cpp:839-843) returned by runOne (cpuLBM.cpp:2334) */
+    LBM_ERR_EQUILIBRIUM = 1,
+    LBM_ERR_INVALID = 2,     /* bad argument or configuration */
+    LBM_ERR_CUDA = 3,        /* CUDA runtime error / no device */
+    LBM_ERR_NOMEM = 4,       /* device allocation failed */
+    LBM_ERR_NONFINITE = 5,   /* the state became NaN/Inf or rho <= 0 */
+    LBM_ERR_BUSY = 6,        /* serving: queue full / no capacity */
+    LBM_ERR_NOT_FOUND = 7,   /* serving: unknown request id */
+    LBM_ERR_TIMEOUT = 8      /* a bounded wait ran out */
+} lbm_status;
+
+/* Storage/compute precision of a handle or batch. */
+enum {
+    LBM_PREC_F64 = 0, /* plain path: FP64 state and arithmetic */
+    LBM_PREC_F32 = 1  /* mixed path: FP32 state and stencil/collision math,
+                         FP64 moment sums and reductions */
+};
+
+/* Configuration: the MAT variables read by cpuLBM::loadInput
+ * (cpuLBM.cpp:113-199), same names and meaning; derived values follow
+ * refineInput/setupVars (cpuLBM.cpp:283-450).  dx_array/dy_array (optional)
+ * give per-column/per-row cell widths as in the OpenCL generator
+ * (CODE/Python/simLB/codeCL.py:100-114); NULL selects uniform dx, dy. */
+typedef struct lbm_config {
+    int RKMETHOD; /* 0 RK1 (IMEX Euler), 1 RK3 (3-stage IMEX), 2 EULER, 3 EULER_EQ */
+    int FMETHOD;  /* 0 NND, 1 WENO5 */
+    double CFL, dtau, tt_tref, tt_time;
+    int steps;
+    double tol;
+    int periodicX, periodicY, mirrorNorth, mirrorSouth, mirrorEast, mirrorWest;
+    double gamma, R, mu, Pr;
+    double dx, dy, Lx, Ly;
+    double rho_ref, p_ref, T_ref, Tc_Tref;
+    const double *dx_array; /* [Nx] or NULL */
+    const double *dy_array; /* [Ny] or NULL */
+} lbm_config;
+
+/* Domain: the property-id map and property tables of loadInput
+ * (cpuLBM.cpp:202-266).  bndArray is in the solver's internal order
+ * BNDARRAY(x,y) = bndArray[x*Ny + y] (i.e. after loadInput's y flip). */
+typedef struct lbm_init {
+    int Nx, Ny, numProps;
+    const int *bndArray;  /* [Nx*Ny] */
+    const int *cellType;  /* [numProps] 0 fluid, 1 permanent, 2 solid */
+    const double *density, *pressure, *temp, *velocityX, *velocityY; /* [numProps] */
+} lbm_init;
+
+typedef struct lbm_info {
+    int Nx, Ny;
+    int step;       /* steps taken (cpuLBM::step) */
+    int nsteps;     /* derived step count (cpuLBM::nsteps) */
+    double dt;      /* cpuLBM::dt */
+    double tstep;   /* step * dt (cpuLBM::tstep) */
+    double residual;/* cpuLBM::residual */
+    int precision;
+    int rkmethod, fmethod;
+    size_t device_bytes; /* device memory held by this handle */
+} lbm_info;
+
+typedef struct lbm_handle lbm_handle;
+
+/* cpuLBM::cpuLBM (cpuLBM.cpp:7-20) + initSim (cpuLBM.cpp:452-462):
+ * derive the run parameters, set f, h to the equilibria of each node's
+ * property and upload.  precision: LBM_PREC_F64 or LBM_PREC_F32. */
+LBM_API lbm_status lbm_create(const lbm_config *cfg, const lbm_init *init, int precision, lbm_handle **out);
+
+/* n_steps x (cpuLBM::updateStepCount + cpuLBM::runOne(want_residual))
+ * (cpuLBM.cpp:771-775, 2284-2335).  Returns LBM_ERR_EQUILIBRIUM where runOne
+ * returns hasFailed = 1 (the failing step still completes, as in the
+ * reference), LBM_ERR_NONFINITE if the state left the finite range.
+ * residual_out (may be NULL) receives cpuLBM::residual after the last step. */
+LBM_API lbm_status lbm_step(lbm_handle *h, int n_steps, int want_residual, double *residual_out);
+
+/* The reference driver loop (main.cpp:32-112, runSimStep without file
+ * output): steps until nsteps is reached, the normalised residual falls to
+ * tol, an equilibrium check fails, or max_steps (<0: unlimited) steps ran.
+ * stop_out: 0 still running, 1 failure, 2 finished.  residual_trace (may be
+ * NULL) receives the per-step residual as main.cpp leaves it. */
+LBM_API lbm_status lbm_run(lbm_handle *h, int max_steps, int *stop_out, double *residual_trace, int trace_len);
+
+/* Public arrays rho_G, u_G, T_G, p_G (cpuLBM.h:93-96) in [x*Ny + y] order,
+ * computed from the current f, h (macroPropShort, cpuLBM.cpp:877-914).
+ * Any pointer may be NULL. */
+LBM_API lbm_status lbm_get_macro(lbm_handle *h, double *rho, double *ux, double *uy, double *T, double *p);
+
+/* f_G, h_G (cpuLBM.h:90-91) in [(x*Ny + y)*13 + i] order; may be NULL. */
+LBM_API lbm_status lbm_get_dist(lbm_handle *h, double *f, double *hh);
+
+/* Replace f, h (same layout); the checkpoint/resume entry point. */
+LBM_API lbm_status lbm_set_dist(lbm_handle *h, const double *f, const double *hh);
+
+LBM_API lbm_status lbm_get_info(lbm_handle *h, lbm_info *info);
+
+/* The CUDA stream (cudaStream_t) the handle's kernels run on. */
+LBM_API void *lbm_stream(lbm_handle *h);
+
+LBM_API void lbm_destroy(lbm_handle *h);
+
+/* Human-readable message of the last failure on the calling thread. */
+LBM_API const char *lbm_last_error(void);
+
+/* -------------------------------------------------------------- batches
+ * Many independent samples (uneven grids, own parameters) advanced
+ * together: every phase is one launch over a packed tile list of all
+ * samples; runs of steps are captured in a CUDA graph.  Samples must share
+ * RKMETHOD where they are stepped together; everything else may differ. */
+typedef struct lbm_batch lbm_batch;
+
+typedef struct lbm_batch_options {
+    int precision;      /* LBM_PREC_F64 / LBM_PREC_F32 */
+    int tile_x, tile_y; /* 0: chosen by the autotuner's table */
+    int use_graph;      /* capture step sequences in CUDA graphs */
+} lbm_batch_options;
+
+LBM_API lbm_status lbm_batch_create(int n, const lbm_config *cfgs, const lbm_init *inits,
+                            const lbm_batch_options *opt, lbm_batch **out);
+/* n_steps steps of every sample; want_residual as runOne(res). */
+LBM_API lbm_status lbm_batch_step(lbm_batch *b, int n_steps, int want_residual);
+/* Per-sample status (lbm_status values) of the steps since the last call. */
+LBM_API lbm_status lbm_batch_status(lbm_batch *b, int *status);
+/* Per-sample residual after the last step with want_residual. */
+LBM_API lbm_status lbm_batch_residuals(lbm_batch *b, double *residual);
+LBM_API lbm_status lbm_batch_get_macro(lbm_batch *b, int sample, double *rho, double *ux, double *uy,
+                               double *T, double *p);
+LBM_API lbm_status lbm_batch_get_dist(lbm_batch *b, int sample, double *f, double *hh);
+LBM_API lbm_status lbm_batch_set_dist(lbm_batch *b, int sample, const double *f, const double *hh);
+/* Lattice updates (nodes) one step of the whole batch performs. */
+LBM_API long long lbm_batch_nodes(lbm_batch *b);
+LBM_API void *lbm_batch_stream(lbm_batch *b);
+LBM_API void lbm_batch_destroy(lbm_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

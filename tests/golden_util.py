@@ -1,0 +1,46 @@
+"""Loading of the committed golden fixtures (tests/golden/*.npz), which the
+unmodified reference solver produced (tests/golden/make_golden.py)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+
+from uq_b200 import workloads as W
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def case_digest(case):
+    h = hashlib.sha256()
+    for k in sorted(case):
+        h.update(k.encode())
+        h.update(np.ascontiguousarray(np.asarray(case[k], dtype=np.float64)).tobytes())
+    return h.hexdigest()[:16]
+
+
+def load(name):
+    """[(case, meta, arrays)] of one fixture file; the case is rebuilt from
+    the recorded builder call and checked against the recorded digest."""
+    z = np.load(os.path.join(GOLDEN, name))
+    metas = json.loads(str(z["meta"]))
+    out = []
+    for k, meta in enumerate(metas):
+        case = W.build(meta["builder"], **meta["kwargs"])
+        assert case_digest(case) == meta["digest"], "case builder drifted for %s[%d]" % (name, k)
+        prefix = "c%d_" % k
+        arrays = {key[len(prefix):]: z[key] for key in z.files if key.startswith(prefix)}
+        out.append((case, meta, arrays))
+    return out
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def rel_max(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))

@@ -1,0 +1,61 @@
+"""The C-ABI library loads and exports every symbol include/uq_lbm.h
+declares; without a GPU, creating a handle fails loudly (no CPU path)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from uq_b200 import native, workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for fn in os.listdir(inc):
+        if fn.endswith(".h"):
+            src = open(os.path.join(inc, fn)).read()
+            names |= set(re.findall(r"^LBM_API[^(]*?\b(lbm_\w+)\s*\(", src, flags=re.M))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(native.LIB_PATH)
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    # and the Python binding covers the same set
+    assert names <= set(native.SIGNATURES), names - set(native.SIGNATURES)
+
+
+def test_create_without_gpu_fails_loudly():
+    import torch
+
+    if torch.cuda.is_available():
+        return
+    from uq_b200.solver import Solver
+
+    case = W.couette(nx=8, ny=8, steps=1)
+    try:
+        Solver(case)
+    except native.LbmError as e:
+        assert e.code == native.LBM_ERR_CUDA
+        assert "CUDA" in str(e) or "device" in str(e)
+    else:
+        raise AssertionError("lbm_create succeeded without a CUDA device")
+
+
+def test_invalid_config_is_rejected():
+    import torch
+
+    if torch.cuda.is_available():
+        return
+    L = native.lib()
+    cfg = native.LbmConfig()
+    ini = native.LbmInit()
+    h = ctypes.c_void_p()
+    assert L.lbm_create(ctypes.byref(cfg), ctypes.byref(ini), 0, ctypes.byref(h)) == native.LBM_ERR_INVALID
+    assert not h.value

@@ -1,0 +1,353 @@
+// Device-side building blocks of the D2Q13 thermal LBM step (sm_100a).
+//
+// Every function restates a piece of the reference FP64 CPU solver
+// CODE/C++/VS2010/simLB/simLB/cpuLBM.cpp (cited per function) for the GPU's
+// structure-of-arrays layout: per sample, 26 planes (f_0..f_12, h_0..h_12),
+// each plane ny rows of `pitch` elements, x fastest.  Templates take the
+// storage type S (double or float) and the compute type C; moment sums are
+// always accumulated in double.
+#pragma once
+
+#include <cstdint>
+
+namespace uqlbm {
+
+constexpr int NQ = 13;
+constexpr int NPL = 26;  // f and h planes
+
+// node-flag byte: cell type in bits 0-1 (0 fluid, 1 permanent, 2 solid);
+// bits 2-5 say whether the 5-point x / y stencil of the node meets a solid
+// node or the domain edge (then the exact boundary-aware stencil runs).
+constexpr uint8_t NF_TYPE = 3;
+constexpr uint8_t NF_SOLX = 4;
+constexpr uint8_t NF_SOLY = 8;
+constexpr uint8_t NF_EDGX = 16;
+constexpr uint8_t NF_EDGY = 32;
+
+// sample flag bits
+constexpr int SF_PERX = 1, SF_PERY = 2, SF_MIRN = 4, SF_MIRS = 8, SF_MIRE = 16, SF_MIRW = 32;
+
+struct SampleParams {
+    int nx, ny, pitch, flags;
+    int rk, fm;          // RKMETHOD, FMETHOD
+    int ntile;           // tiles of this sample in the full tile list
+    int first_tile;
+    long long state_off; // element offset of plane 0 in every state buffer
+    long long plane;     // elements per plane
+    long long node_off;  // offset into per-node arrays
+    int xoff, yoff;      // offsets into the per-column / per-row spacing tables
+    double R, bR, K, Tc, inv_sRTc, RTc, mu, Pr, dt, c;
+};
+
+struct Tile {
+    int sample;
+    int x0, y0;
+    int gid;  // index of the tile in the batch's full tile list
+};
+
+// lattice (setupVars, cpuLBM.cpp:376-388) in units of c, its signs, and the
+// reflection maps of mirIndex (cpuLBM.cpp:1147-1169)
+__constant__ int c_EX[NQ] = {0, 1, 0, -1, 0, 1, -1, -1, 1, 2, 0, -2, 0};
+__constant__ int c_EY[NQ] = {0, 0, 1, 0, -1, 1, 1, -1, -1, 0, 2, 0, -2};
+__constant__ int c_MIR_NS[NQ] = {0, 1, 4, 3, 2, 8, 7, 6, 5, 9, 12, 11, 10};
+__constant__ int c_MIR_EW[NQ] = {0, 3, 2, 1, 4, 6, 5, 8, 7, 11, 10, 9, 12};
+
+__device__ __forceinline__ int isgn(int a) { return (a > 0) - (a < 0); }
+
+// ------------------------------------------------------------ equilibria
+// equilibrium2D (cpuLBM.cpp:785-844) with the polynomials of
+// inlineFunctions.cpp:10-61, evaluated per symmetry family.  Normalised
+// u, v, T are u/sqrt(R Tc), v/sqrt(R Tc), T/Tc; with a = u^2, c = v^2:
+//   f0      = 1 + 5/2 T^2 + 5/2 T (a + c - 1) + (a^2 + c^2)/4 + a c - 5/4 (a + c)
+//   f1, f3  = E1(u, v) +- O1(u, v);   f2, f4 = E1(v, u) +- O1(v, u)
+//   f5..f8  = (T + a +- u)(T + c +- v) / 4
+//   f9, f11 = E9(u) +- O9(u);         f10, f12 = E9(v) +- O9(v)
+// times rho, and the h families times rho R Tc.
+template <class C>
+struct EqState {
+    C rho, u, v, T, K, rRTc;  // normalised velocity/temperature
+};
+
+template <class C>
+__device__ __forceinline__ EqState<C> eq_state(double rho, double ux, double uy, double T, const SampleParams &sp)
+{
+    EqState<C> e;
+    e.rho = (C)rho;
+    e.u = (C)(ux * sp.inv_sRTc);
+    e.v = (C)(uy * sp.inv_sRTc);
+    e.T = (C)(T / sp.Tc);
+    e.K = (C)sp.K;
+    e.rRTc = (C)(rho * sp.RTc);
+    return e;
+}
+
+// family 0: direction 0
+template <class C>
+__device__ __forceinline__ void eq_fam0(const EqState<C> &q, C &f0, C &h0)
+{
+    const C a = q.u * q.u, c = q.v * q.v, s2 = a + c, pc = a * c, T = q.T, T2 = T * T, T3 = T2 * T, K = q.K;
+    f0 = q.rho * (C(1) + C(2.5) * T2 + C(2.5) * T * (s2 - C(1)) + C(0.25) * (a * a + c * c) + pc - C(1.25) * s2);
+    h0 = q.rRTc * (T3 * (C(1.25) * K + C(20.0 / 3.0)) + T2 * ((C(1.25) * K + C(11.25)) * s2 - C(1.25) * K - C(5))
+                   + T * (C(0.125) * K * (s2 * s2 + C(2) * pc) - C(0.625) * K * s2 + C(0.5) * K + C(2.5) * s2 * s2
+                          + C(2.5) * pc - C(5) * s2 + C(1))
+                   + s2 * s2 * s2 * C(0.125) + C(0.25) * pc * s2 - C(0.625) * s2 * s2 + C(0.5) * s2);
+}
+
+// family 1: directions 1..4 (out[0..3] = f1..f4, h1..h4)
+template <class C>
+__device__ __forceinline__ void eq_fam1(const EqState<C> &q, C *f, C *h)
+{
+    const C T = q.T, T2 = T * T, T3 = T2 * T, K = q.K;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const C U = k == 0 ? q.u : q.v;
+        const C W = k == 0 ? q.v : q.u;
+        const C A = U * U, Cc = W * W;
+        C E = -T2 + T * (C(2.0 / 3.0) - C(1.5) * A - C(0.5) * Cc) + C(2.0 / 3.0) * A - A * A * C(1.0 / 6.0) - C(0.5) * A * Cc;
+        C O = U * (C(2.0 / 3.0) - T - A * C(1.0 / 6.0) - C(0.5) * Cc);
+        f[k] = q.rho * (E + O);
+        f[k + 2] = q.rho * (E - O);
+        E = T3 * (C(-0.5) * K - C(8.0 / 3.0))
+            + T2 * (-(C(0.75) * K + C(6.5)) * A - (C(0.25) * K + C(2.5)) * Cc + K * C(1.0 / 3.0) + C(4.0 / 3.0))
+            + T * (-(K * C(1.0 / 12.0) + C(19.0 / 12.0)) * A * A - (C(0.25) * K + C(3.5)) * A * Cc
+                   + (K * C(1.0 / 3.0) + C(7.0 / 3.0)) * A - C(0.25) * Cc * Cc + Cc * C(1.0 / 3.0))
+            - A * A * A * C(1.0 / 12.0) - A * A * Cc * C(1.0 / 3.0) + A * A * C(1.0 / 3.0) - C(0.25) * A * Cc * Cc
+            + A * Cc * C(1.0 / 3.0);
+        O = U * (T2 * (C(-0.5) * K - C(3))
+                 + T * (-(K * C(1.0 / 12.0) + C(7.0 / 6.0)) * A - (C(0.25) * K + C(2.5)) * Cc + K * C(1.0 / 3.0) + C(4.0 / 3.0))
+                 - A * A * C(1.0 / 12.0) - A * Cc * C(1.0 / 3.0) + A * C(1.0 / 3.0) - C(0.25) * Cc * Cc + Cc * C(1.0 / 3.0));
+        h[k] = q.rRTc * (E + O);
+        h[k + 2] = q.rRTc * (E - O);
+    }
+}
+
+// family 5: directions 5..8
+template <class C>
+__device__ __forceinline__ void eq_fam5(const EqState<C> &q, C *f, C *h)
+{
+    const C u = q.u, v = q.v, a = u * u, c = v * v, s2 = a + c, pc = a * c, T = q.T, T2 = T * T, T3 = T2 * T, K = q.K;
+    const C Ap = T + a + u, Am = T + a - u, Bp = T + c + v, Bm = T + c - v, r4 = C(0.25) * q.rho;
+    f[0] = r4 * (Ap * Bp);
+    f[1] = r4 * (Am * Bp);
+    f[2] = r4 * (Am * Bm);
+    f[3] = r4 * (Ap * Bm);
+    const C k8 = C(0.125) * K;
+    const C EE = T3 * (k8 + C(2.0 / 3.0)) + T2 * (k8 + C(1.125)) * s2 + T * ((k8 + C(1.5)) * pc + C(0.125) * (a * a + c * c))
+                 + C(0.125) * pc * s2;
+    const C OE = u * (T2 * (k8 + C(0.75)) + T * ((k8 + C(1.125)) * c + C(0.125) * a) + C(0.125) * c * s2);
+    const C EO = v * (T2 * (k8 + C(0.75)) + T * ((k8 + C(1.125)) * a + C(0.125) * c) + C(0.125) * a * s2);
+    const C OO = u * v * (T * (k8 + C(0.75)) + C(0.125) * s2);
+    h[0] = q.rRTc * (EE + OE + EO + OO);
+    h[1] = q.rRTc * (EE - OE + EO - OO);
+    h[2] = q.rRTc * (EE - OE - EO + OO);
+    h[3] = q.rRTc * (EE + OE - EO - OO);
+}
+
+// family 9: directions 9..12
+template <class C>
+__device__ __forceinline__ void eq_fam9(const EqState<C> &q, C *f, C *h)
+{
+    const C T = q.T, T2 = T * T, T3 = T2 * T, K = q.K;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const C U = k == 0 ? q.u : q.v;
+        const C W = k == 0 ? q.v : q.u;
+        const C A = U * U, Cc = W * W;
+        C E = C(0.125) * T2 + T * (C(0.25) * A - C(1.0 / 24.0)) + (A * A - A) * C(1.0 / 24.0);
+        C O = U * (C(0.25) * T + (A - C(1)) * C(1.0 / 12.0));
+        f[k] = q.rho * (E + O);
+        f[k + 2] = q.rho * (E - O);
+        E = T3 * (K * C(1.0 / 16.0) + C(1.0 / 3.0))
+            + T2 * ((C(0.125) * K + C(17.0 / 16.0)) * A + Cc * C(1.0 / 16.0) - K * C(1.0 / 48.0) - C(1.0 / 12.0))
+            + T * ((K * C(1.0 / 48.0) + C(1.0 / 3.0)) * A * A - (K * C(1.0 / 48.0) + C(7.0 / 48.0)) * A + C(0.125) * A * Cc
+                   - Cc * C(1.0 / 48.0))
+            + (A * A * A + A * A * Cc - A * A - A * Cc) * C(1.0 / 48.0);
+        O = U * (T2 * (C(0.125) * K + C(0.75)) + T * ((K * C(1.0 / 24.0) + C(11.0 / 24.0)) * A - K * C(1.0 / 24.0) - C(1.0 / 6.0) + C(0.125) * Cc)
+                 + (A * A + A * Cc - A - Cc) * C(1.0 / 24.0));
+        h[k] = q.rRTc * (E + O);
+        h[k + 2] = q.rRTc * (E - O);
+    }
+}
+
+// all 26 values (init, pointwise stages)
+template <class C>
+__device__ __forceinline__ void eq_all(const EqState<C> &q, C *f, C *h)
+{
+    eq_fam0(q, f[0], h[0]);
+    eq_fam1(q, f + 1, h + 1);
+    eq_fam5(q, f + 5, h + 5);
+    eq_fam9(q, f + 9, h + 9);
+}
+
+// ---------------------------------------------------------------- moments
+// macroProp/macroPropShort (cpuLBM.cpp:877-970): FP64 sums over the node's
+// 13 f and 13 h values; tau_f = mu/p, tau_h = tau_f/Pr,
+// tau_hf = tau_h tau_f / (tau_f - tau_h) (cpuLBM.cpp:952-955).
+struct Macro {
+    double rho, ux, uy, T, p, tf, th, thf;
+};
+
+__device__ __forceinline__ Macro macro_from_sums(double r, double rux, double ruy, double sh, const SampleParams &sp)
+{
+    Macro m;
+    m.rho = r;
+    m.ux = rux / r;
+    m.uy = ruy / r;
+    const double usq = m.ux * m.ux + m.uy * m.uy;
+    m.T = 2.0 * (sh / r - usq / 2.0) / sp.bR;
+    m.p = r * sp.R * m.T;
+    m.tf = sp.mu / m.p;
+    m.th = m.tf / sp.Pr;
+    m.thf = (m.th * m.tf) / (m.tf - m.th);
+    return m;
+}
+
+// ---------------------------------------------------------- index and BCs
+// index (cpuLBM.cpp:1033-1113): periodic wrap, mirror (-i-1 / 2N-i-1 with a
+// reflection flag) or zeroth-order extrapolation (clamp).
+__device__ __forceinline__ int bc_index(const SampleParams &sp, int i, int pm, int axis, int &mir)
+{
+    i += pm;
+    mir = 0;
+    const int N = axis == 0 ? sp.nx : sp.ny;
+    if (i < 0) {
+        if (sp.flags & (axis == 0 ? SF_PERX : SF_PERY)) i = N + i;
+        else if (sp.flags & (axis == 0 ? SF_MIRW : SF_MIRS)) { i = -i - 1; mir = 1; }
+        else i = 0;
+    } else if (i > N - 1) {
+        if (sp.flags & (axis == 0 ? SF_PERX : SF_PERY)) i = i - N;
+        else if (sp.flags & (axis == 0 ? SF_MIRE : SF_MIRN)) { i = 2 * N - i - 1; mir = 1; }
+        else i = N - 1;
+    }
+    return i;
+}
+
+// -------------------------------------------------------------- NND, WENO5
+// minmod with the reference's case order (cpuLBM.cpp:1130-1145)
+template <class C>
+__device__ __forceinline__ C minmod(C a, C b)
+{
+    C out = C(0);
+    if (fabs(a) < fabs(b) && a * b > C(0)) out = a;
+    else if (fabs(b) < fabs(a) && a * b > C(0)) out = b;
+    else if (a == b) out = a;
+    return out;
+}
+
+// NND (cpuLBM.cpp:1328-1356) on the 3 upwind-ordered values s0, s1, s2
+template <class C>
+__device__ __forceinline__ C nnd3(C ae, C s0, C s1, C s2)
+{
+    const C c = ae * s1;
+    return c + C(0.5) * minmod<C>(ae * s2 - c, c - ae * s0);
+}
+
+// WENO5 (cpuLBM.cpp:1358-1403): Jiang-Shu indicators, linear weights
+// 1/10, 6/10, 3/10, epsilon 1e-6, on |e| times the upwind-ordered values.
+template <class C>
+__device__ __forceinline__ C weno5(C ae, C s0, C s1, C s2, C s3, C s4)
+{
+    const C q0 = ae * s0, q1 = ae * s1, q2 = ae * s2, q3 = ae * s3, q4 = ae * s4;
+    const C d0 = q0 - C(2) * q1 + q2, d1 = q1 - C(2) * q2 + q3, d2 = q2 - C(2) * q3 + q4;
+    const C l0 = q0 - C(4) * q1 + C(3) * q2, l1 = q1 - q3, l2 = C(3) * q2 - C(4) * q3 + q4;
+    const C b0 = C(13.0 / 12.0) * d0 * d0 + C(0.25) * l0 * l0;
+    const C b1 = C(13.0 / 12.0) * d1 * d1 + C(0.25) * l1 * l1;
+    const C b2 = C(13.0 / 12.0) * d2 * d2 + C(0.25) * l2 * l2;
+    const C g0 = C(1) / (C(1e-6) + b0), g1 = C(1) / (C(1e-6) + b1), g2 = C(1) / (C(1e-6) + b2);
+    const C w0 = C(0.1) * g0 * g0, w1 = C(0.6) * g1 * g1, w2 = C(0.3) * g2 * g2;
+    const C ws = w0 + w1 + w2;
+    const C r0 = (C(2) * q0 - C(7) * q1 + C(11) * q2) * C(1.0 / 6.0);
+    const C r1 = (-q1 + C(5) * q2 + C(2) * q3) * C(1.0 / 6.0);
+    const C r2 = (C(2) * q2 + C(5) * q3 - q4) * C(1.0 / 6.0);
+    return (w0 * r0 + w1 * r1 + w2 * r2) / ws;
+}
+
+// view of one sample's stage buffer and node flags
+template <class S>
+struct StageView {
+    const S *__restrict__ st;        // plane 0 of the sample in the stage buffer
+    const uint8_t *__restrict__ nf;  // node flags of the sample
+    long long plane;
+    int pitch;
+};
+
+template <class S>
+__device__ __forceinline__ S ldv(const StageView<S> &v, int p, int x, int y)
+{
+    return __ldg(v.st + (long long)p * v.plane + (long long)y * v.pitch + x);
+}
+
+// Exact stencil + reconstruction (stencil, cpuLBM.cpp:1171-1326, then NND/
+// WENO5) for the flux of plane p along `axis` at (x, y): boundary-aware
+// indices with reflections, and the linear extrapolation 2 f(m1) - f(m2)
+// over the first solid/fluid edge met by the stencil.
+template <class S, class C>
+__device__ C flux_exact(const SampleParams &sp, const StageView<S> &v, int x, int y, int p, int axis)
+{
+    const int i = p < NQ ? p : p - NQ, pb = p - i;
+    const int e = axis == 0 ? isgn(c_EX[i]) : isgn(c_EY[i]);
+    if (e == 0) return C(0);
+    const C ae = (C)(sp.c * (double)abs(axis == 0 ? c_EX[i] : c_EY[i]));
+    const int L = sp.fm ? 5 : 3, low = (L - 1) / 2;
+    const int pos = axis == 0 ? x : y;
+    const int j1 = pos - e * low;
+    C S5[5];
+    int sld[5];
+    int any = 0;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        if (j < L) {
+            int m;
+            const int r = bc_index(sp, j1, e * j, axis, m);
+            const int pp = m ? pb + (axis == 0 ? c_MIR_EW[i] : c_MIR_NS[i]) : p;
+            const int xr = axis == 0 ? r : x, yr = axis == 0 ? y : r;
+            S5[j] = (C)ldv(v, pp, xr, yr);
+            sld[j] = (v.nf[(long long)yr * v.pitch + xr] & NF_TYPE) == 2;
+            any |= sld[j];
+        }
+    }
+    if (any) {
+        int diff = 0, jj = 0, pe = 0, m;
+        for (int j = 0; j < L - 1; ++j) {
+            diff = sld[j] - sld[j + 1];
+            if (diff > 0) { jj = j; pe = bc_index(sp, j1, e * j, axis, m); break; }
+            if (diff < 0) { jj = j + 1; pe = bc_index(sp, j1, e * (j + 1), axis, m); break; }
+        }
+        const int r1 = bc_index(sp, pe, e * diff, axis, m);
+        const int r2 = bc_index(sp, pe, e * 2 * diff, axis, m);
+        const C v1 = axis == 0 ? (C)ldv(v, p, r1, y) : (C)ldv(v, p, x, r1);
+        const C v2 = axis == 0 ? (C)ldv(v, p, r2, y) : (C)ldv(v, p, x, r2);
+        const C ext = C(2) * v1 - v2;
+        // S5[jj] = ext; S5[jj - diff] = ext when inside the stencil
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+            if (j < L && (j == jj || (j == jj - diff))) S5[j] = ext;
+    }
+    if (sp.fm) return weno5<C>(ae, S5[0], S5[1], S5[2], S5[3], S5[4]);
+    return nnd3<C>(ae, S5[0], S5[1], S5[2]);
+}
+
+// Outgoing face flux of plane p along `axis` at a non-solid node; the fast
+// path (no solid, no domain edge within the stencil) reads the five
+// neighbours directly.
+template <class S, class C>
+__device__ __forceinline__ C flux_axis(const SampleParams &sp, const StageView<S> &v, int x, int y, int p, int axis,
+                                       uint8_t nflag)
+{
+    const int i = p < NQ ? p : p - NQ;
+    const int ev = axis == 0 ? c_EX[i] : c_EY[i];
+    if (ev == 0) return C(0);
+    const uint8_t slow = axis == 0 ? (NF_SOLX | NF_EDGX) : (NF_SOLY | NF_EDGY);
+    if (nflag & slow) return flux_exact<S, C>(sp, v, x, y, p, axis);
+    const int e = ev > 0 ? 1 : -1;
+    const C ae = (C)(sp.c * (double)abs(ev));
+    const long long stride = axis == 0 ? (long long)e : (long long)e * v.pitch;
+    const S *c0 = v.st + (long long)p * v.plane + (long long)y * v.pitch + x;
+    if (sp.fm) {
+        return weno5<C>(ae, (C)__ldg(c0 - 2 * stride), (C)__ldg(c0 - stride), (C)__ldg(c0), (C)__ldg(c0 + stride),
+                        (C)__ldg(c0 + 2 * stride));
+    }
+    return nnd3<C>(ae, (C)__ldg(c0 - stride), (C)__ldg(c0), (C)__ldg(c0 + stride));
+}
+
+}  // namespace uqlbm

@@ -1,0 +1,775 @@
+// Host engine and C ABI (include/uq_lbm.h) of the D2Q13 thermal LBM step.
+//
+// A Batch holds any number of samples (a single lbm_handle is a batch of
+// one).  Their state lives on the device as structure-of-arrays planes; one
+// step is the phase sequence described in lbm_kernels.cu, launched over
+// packed tile lists and, when enabled, replayed from a captured CUDA graph.
+// Derived run parameters follow cpuLBM::refineInput / setupVars
+// (CODE/C++/VS2010/simLB/simLB/cpuLBM.cpp:283-450) and the step driver
+// follows runSimStep (main.cpp:32-112).
+#include "lbm_device.cuh"
+#include "lbm_kernels.h"
+#include "../../include/uq_lbm.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace uqlbm {
+
+static thread_local std::string g_last_error;
+
+struct LbmError : std::runtime_error {
+    lbm_status code;
+    LbmError(lbm_status c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define CU(call)                                                                                          \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess)                                                                            \
+            throw LbmError(e_ == cudaErrorMemoryAllocation ? LBM_ERR_NOMEM : LBM_ERR_CUDA,                \
+                           std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+    } while (0)
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count)
+    {
+        free();
+        if (count == 0) return;
+        CU(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void upload(const std::vector<T> &v, cudaStream_t s)
+    {
+        alloc(v.size());
+        if (!v.empty()) CU(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void free()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { free(); }
+};
+
+// Host-side description of one sample after refineInput / setupVars.
+struct HostSample {
+    int nx = 0, ny = 0, rk = 1, fm = 1;
+    int flags = 0;
+    double R = 1, b = 5, K = 3, Tc = 1, c = 1, mu = 0, Pr = 1, dt = 0, tol = 0;
+    int nsteps = 0;
+    std::vector<double> dx, dy;
+    std::vector<uint8_t> type;  // [y*nx + x]
+    std::vector<double> rho0, ux0, uy0, T0;  // [y*nx + x] initial node state
+    // driver state (cpuLBM::step, residual, initRes, resNorm; main.cpp:34-70)
+    int step = 0;
+    double residual = 1, resNorm = 0, initRes[100] = {0};
+};
+
+static int host_bc_index(const HostSample &s, int i, int pm, int axis, int &mir)
+{
+    i += pm;
+    mir = 0;
+    const int N = axis == 0 ? s.nx : s.ny;
+    if (i < 0) {
+        if (s.flags & (axis == 0 ? SF_PERX : SF_PERY)) i = N + i;
+        else if (s.flags & (axis == 0 ? SF_MIRW : SF_MIRS)) { i = -i - 1; mir = 1; }
+        else i = 0;
+    } else if (i > N - 1) {
+        if (s.flags & (axis == 0 ? SF_PERX : SF_PERY)) i = i - N;
+        else if (s.flags & (axis == 0 ? SF_MIRE : SF_MIRN)) { i = 2 * N - i - 1; mir = 1; }
+        else i = N - 1;
+    }
+    return i;
+}
+
+// refineInput (cpuLBM.cpp:283-358) + setupVars (cpuLBM.cpp:360-450)
+static HostSample derive(const lbm_config &c, const lbm_init &in)
+{
+    HostSample s;
+    if (in.Nx < 3 || in.Ny < 3) throw LbmError(LBM_ERR_INVALID, "Nx and Ny must be at least 3");
+    if (c.RKMETHOD < 0 || c.RKMETHOD > 3) throw LbmError(LBM_ERR_INVALID, "RKMETHOD must be 0..3");
+    if (c.FMETHOD < 0 || c.FMETHOD > 1) throw LbmError(LBM_ERR_INVALID, "FMETHOD must be 0 (NND) or 1 (WENO5)");
+    if (!in.bndArray || !in.cellType || !in.density || !in.pressure || !in.temp || !in.velocityX || !in.velocityY ||
+        in.numProps < 1)
+        throw LbmError(LBM_ERR_INVALID, "lbm_init tables missing");
+    if (!(c.gamma > 1.0) || !(c.R > 0.0)) throw LbmError(LBM_ERR_INVALID, "gamma must exceed 1 and R be positive");
+    const int Nx = in.Nx, Ny = in.Ny;
+    s.nx = Nx;
+    s.ny = Ny;
+    s.rk = c.RKMETHOD;
+    s.fm = c.FMETHOD;
+    s.flags = (c.periodicX > 0 ? SF_PERX : 0) | (c.periodicY > 0 ? SF_PERY : 0) | (c.mirrorNorth > 0 ? SF_MIRN : 0) |
+              (c.mirrorSouth > 0 ? SF_MIRS : 0) | (c.mirrorEast > 0 ? SF_MIRE : 0) | (c.mirrorWest > 0 ? SF_MIRW : 0);
+    s.R = c.R;
+    s.mu = c.mu;
+    s.Pr = c.Pr;
+    s.tol = c.tol;
+    double dx = c.dx, dy = c.dy, Lx = c.Lx, Ly = c.Ly;
+    if (dx == 0) dx = Lx / ((double)Nx - 1); else Lx = dx * (Nx - 1);
+    if (dy == 0 && Ly != 0) dy = Ly / ((double)Ny - 1);
+    else if (dy == 0 && Ly == 0) { dy = dx; Ly = dy * (Ny - 1); }
+    else Ly = dy * (Ny - 1);
+    double rho_ref = c.rho_ref, p_ref = c.p_ref, T_ref = c.T_ref;
+    if (rho_ref == 0) rho_ref = p_ref / (c.R * T_ref);
+    else if (p_ref == 0) p_ref = rho_ref * c.R * T_ref;
+    else if (T_ref == 0) T_ref = p_ref / (rho_ref * c.R);
+    s.dx.resize(Nx);
+    s.dy.resize(Ny);
+    const bool nonuni = c.dx_array || c.dy_array;
+    double mind = std::min(dx, dy);
+    if (nonuni) mind = INFINITY;
+    for (int x = 0; x < Nx; ++x) {
+        s.dx[x] = c.dx_array ? c.dx_array[x] : dx;
+        if (nonuni) mind = std::min(mind, s.dx[x]);
+    }
+    for (int y = 0; y < Ny; ++y) {
+        s.dy[y] = c.dy_array ? c.dy_array[y] : dy;
+        if (nonuni) mind = std::min(mind, s.dy[y]);
+    }
+    s.b = 2 / (c.gamma - 1);
+    s.K = s.b - 2;
+    s.Tc = c.Tc_Tref * T_ref;
+    const double tau_ref = c.mu / p_ref;
+    const double u_ref = std::sqrt(c.R * T_ref);
+    const double t_ref = std::max(Lx, Ly) / u_ref;
+    s.c = std::sqrt(c.R * s.Tc);
+    s.dt = c.dtau == 0 ? (c.CFL * mind) / (2 * s.c) : c.dtau * tau_ref;
+    if (!(s.dt > 0) || !std::isfinite(s.dt)) throw LbmError(LBM_ERR_INVALID, "derived dt is not positive");
+    double ttotal = 0;
+    int need = 0;
+    if (c.tt_tref > 0) { ttotal = c.tt_tref * t_ref; need = 1; }
+    else if (c.tt_time > 0) { ttotal = c.tt_time; need = 1; }
+    else if (c.steps > 0) s.nsteps = c.steps;
+    else if (c.tol > 0) s.nsteps = 0;
+    if (need) s.nsteps = (int)std::ceil(ttotal / s.dt);
+
+    // property tables completed as refineInput does; per-node initial state
+    const int np = in.numProps;
+    std::vector<double> prho(np), pT(np);
+    for (int r = 0; r < np; ++r) {
+        double rho = in.density[r], p = in.pressure[r], T = in.temp[r];
+        if (rho == 0) rho = p / (c.R * T);
+        else if (p == 0) p = rho * c.R * T;
+        else if (T == 0) T = p / (rho * c.R);
+        prho[r] = rho;
+        pT[r] = T;
+        if (in.cellType[r] < 0 || in.cellType[r] > 2) throw LbmError(LBM_ERR_INVALID, "cellType must be 0, 1 or 2");
+    }
+    const size_t N = (size_t)Nx * Ny;
+    s.type.resize(N);
+    s.rho0.resize(N);
+    s.ux0.resize(N);
+    s.uy0.resize(N);
+    s.T0.resize(N);
+    for (int x = 0; x < Nx; ++x)
+        for (int y = 0; y < Ny; ++y) {
+            const int id = in.bndArray[(size_t)x * Ny + y];
+            if (id < 0 || id >= np) throw LbmError(LBM_ERR_INVALID, "bndArray holds an unknown property id");
+            const size_t k = (size_t)y * Nx + x;
+            s.type[k] = (uint8_t)in.cellType[id];
+            s.rho0[k] = prho[id];
+            s.ux0[k] = in.velocityX[id];
+            s.uy0[k] = in.velocityY[id];
+            s.T0[k] = pT[id];
+        }
+    return s;
+}
+
+static int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+}  // namespace uqlbm
+
+using namespace uqlbm;
+
+struct lbm_batch {
+    int prec = LBM_PREC_F64;
+    int tx = 32, ty = 8;
+    bool use_graph = true;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<HostSample> hs;
+    std::vector<SampleParams> sp;
+    std::vector<Tile> tiles_all, tiles_rk3;
+    std::vector<WallNode> walls_all, walls_rk3;
+    std::vector<int> tile_first, tile_count;
+    long long total_state = 0, total_nodes = 0, lattice_nodes = 0;
+    size_t max_nodes = 0;
+    bool any_rk3 = false, any_other = false;
+
+    DevBuf<unsigned char> state, buf2, buf3, alpha;  // typed by precision
+    DevBuf<uint8_t> nflags;
+    DevBuf<double> told, partial, residual, tdx, tdy, dxv, dyv, scratch;
+    DevBuf<int> status, d_tile_first, d_tile_count;
+    DevBuf<SampleParams> d_sp;
+    DevBuf<Tile> d_tiles_all, d_tiles_rk3;
+    DevBuf<WallNode> d_walls_all, d_walls_rk3;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [want_residual]
+    std::vector<int> host_status;
+    std::vector<double> host_residual;
+
+    size_t elem() const { return prec == LBM_PREC_F64 ? 8 : 4; }
+
+    ~lbm_batch()
+    {
+        for (auto &g : graph)
+            if (g) cudaGraphExecDestroy(g);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <class S>
+    KArgs<S> args(int want_res) const
+    {
+        KArgs<S> a{};
+        a.samples = d_sp.p;
+        a.tiles = d_tiles_all.p;
+        a.ntiles = (int)tiles_all.size();
+        a.tx = tx;
+        a.ty = ty;
+        a.state = reinterpret_cast<S *>(state.p);
+        a.buf2 = reinterpret_cast<S *>(buf2.p);
+        a.buf3 = reinterpret_cast<S *>(buf3.p);
+        a.nflags = nflags.p;
+        a.alpha_raw = alpha.p;
+        a.told = told.p;
+        a.partial = partial.p;
+        a.status = status.p;
+        a.tdx = tdx.p;
+        a.tdy = tdy.p;
+        a.dxv = dxv.p;
+        a.dyv = dyv.p;
+        a.want_residual = want_res;
+        a.eq_tol = 1e-6;
+        return a;
+    }
+
+    void build(int n, const lbm_config *cfgs, const lbm_init *inits, const lbm_batch_options *opt)
+    {
+        if (n < 1 || !cfgs || !inits) throw LbmError(LBM_ERR_INVALID, "empty batch");
+        prec = opt ? opt->precision : LBM_PREC_F64;
+        if (prec != LBM_PREC_F64 && prec != LBM_PREC_F32) throw LbmError(LBM_ERR_INVALID, "unknown precision");
+        if (opt && opt->tile_x > 0) tx = opt->tile_x;
+        if (opt && opt->tile_y > 0) ty = opt->tile_y;
+        if (tx * ty > 256 || tx < 1 || ty < 1 || tx * ty % 32 != 0)
+            throw LbmError(LBM_ERR_INVALID, "tile must hold a multiple of 32 and at most 256 nodes");
+        use_graph = opt ? opt->use_graph != 0 : true;
+        hs.reserve(n);
+        for (int k = 0; k < n; ++k) hs.push_back(derive(cfgs[k], inits[k]));
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+            throw LbmError(LBM_ERR_CUDA, "no CUDA device available (this library has no CPU path)");
+        CU(cudaGetDevice(&device));
+        CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+
+        // layout: per sample 26 planes of ny x pitch, pitch a multiple of 32
+        std::vector<double> v_tdx, v_tdy, v_dx, v_dy;
+        std::vector<uint8_t> flags;
+        long long state_off = 0, node_off = 0;
+        for (int k = 0; k < n; ++k) {
+            const HostSample &h = hs[k];
+            SampleParams p{};
+            p.nx = h.nx;
+            p.ny = h.ny;
+            p.pitch = round_up(h.nx, 32);
+            p.flags = h.flags;
+            p.rk = h.rk;
+            p.fm = h.fm;
+            p.plane = (long long)p.ny * p.pitch;
+            p.state_off = state_off;
+            p.node_off = node_off;
+            p.xoff = (int)v_tdx.size();
+            p.yoff = (int)v_tdy.size();
+            p.R = h.R;
+            p.bR = h.b * h.R;
+            p.K = h.K;
+            p.Tc = h.Tc;
+            p.inv_sRTc = 1.0 / std::sqrt(h.R * h.Tc);
+            p.RTc = h.R * h.Tc;
+            p.mu = h.mu;
+            p.Pr = h.Pr;
+            p.dt = h.dt;
+            p.c = h.c;
+            for (int x = 0; x < h.nx; ++x) { v_tdx.push_back(h.dt / h.dx[x]); v_dx.push_back(h.dx[x]); }
+            for (int y = 0; y < h.ny; ++y) { v_tdy.push_back(h.dt / h.dy[y]); v_dy.push_back(h.dy[y]); }
+            state_off += NPL * p.plane;
+            node_off += p.plane;
+            lattice_nodes += (long long)h.nx * h.ny;
+            max_nodes = std::max(max_nodes, (size_t)h.nx * h.ny);
+            // node flags
+            flags.resize(node_off, 0);
+            for (int y = 0; y < h.ny; ++y)
+                for (int x = 0; x < h.nx; ++x) {
+                    uint8_t fl = h.type[(size_t)y * h.nx + x];
+                    int m;
+                    for (int d = -2; d <= 2; ++d) {
+                        const int xr = host_bc_index(h, x, d, 0, m);
+                        const int yr = host_bc_index(h, y, d, 1, m);
+                        if (h.type[(size_t)y * h.nx + xr] == 2) fl |= NF_SOLX;
+                        if (h.type[(size_t)yr * h.nx + x] == 2) fl |= NF_SOLY;
+                    }
+                    if (x < 2 || x > h.nx - 3) fl |= NF_EDGX;
+                    if (y < 2 || y > h.ny - 3) fl |= NF_EDGY;
+                    flags[p.node_off + (long long)y * p.pitch + x] = fl;
+                }
+            // tiles
+            p.first_tile = (int)tiles_all.size();
+            for (int y0 = 0; y0 < h.ny; y0 += ty)
+                for (int x0 = 0; x0 < h.nx; x0 += tx) {
+                    Tile t{k, x0, y0, (int)tiles_all.size()};
+                    tiles_all.push_back(t);
+                    if (h.rk == 1) tiles_rk3.push_back(t);
+                }
+            p.ntile = (int)tiles_all.size() - p.first_tile;
+            tile_first.push_back(p.first_tile);
+            tile_count.push_back(p.ntile);
+            // wall nodes: solid with a non-solid 4-neighbour (wallFluxes' test)
+            static const int wx[4] = {-1, 1, 0, 0}, wy[4] = {0, 0, -1, 1};
+            for (int y = 0; y < h.ny; ++y)
+                for (int x = 0; x < h.nx; ++x) {
+                    if (h.type[(size_t)y * h.nx + x] != 2) continue;
+                    bool adj = false;
+                    for (int j = 0; j < 4; ++j) {
+                        const int xm = host_bc_index(h, x, wx[j], 0, m_dummy());
+                        const int ym = host_bc_index(h, y, wy[j], 1, m_dummy());
+                        if (h.type[(size_t)ym * h.nx + xm] < 2) adj = true;
+                    }
+                    if (adj) {
+                        walls_all.push_back(WallNode{k, x, y, 0});
+                        if (h.rk == 1) walls_rk3.push_back(WallNode{k, x, y, 0});
+                    }
+                }
+            if (h.rk == 1) any_rk3 = true; else any_other = true;
+            sp.push_back(p);
+        }
+        total_state = state_off;
+        total_nodes = node_off;
+
+        state.alloc(total_state * elem());
+        buf2.alloc(total_state * elem());
+        buf3.alloc(total_state * elem());
+        alpha.alloc(total_nodes * elem());
+        CU(cudaMemsetAsync(state.p, 0, state.n, stream));
+        CU(cudaMemsetAsync(buf2.p, 0, buf2.n, stream));
+        CU(cudaMemsetAsync(buf3.p, 0, buf3.n, stream));
+        CU(cudaMemsetAsync(alpha.p, 0, alpha.n, stream));
+        nflags.upload(flags, stream);
+        told.alloc(total_nodes);
+        partial.alloc(tiles_all.size());
+        residual.alloc(n);
+        status.alloc(n);
+        CU(cudaMemsetAsync(status.p, 0, n * sizeof(int), stream));
+        tdx.upload(v_tdx, stream);
+        tdy.upload(v_tdy, stream);
+        dxv.upload(v_dx, stream);
+        dyv.upload(v_dy, stream);
+        d_sp.upload(sp, stream);
+        d_tiles_all.upload(tiles_all, stream);
+        d_tiles_rk3.upload(tiles_rk3, stream);
+        d_walls_all.upload(walls_all, stream);
+        d_walls_rk3.upload(walls_rk3, stream);
+        d_tile_first.upload(tile_first, stream);
+        d_tile_count.upload(tile_count, stream);
+        scratch.alloc(std::max<size_t>(5 * max_nodes, 2 * 13 * max_nodes));
+        host_status.assign(n, 0);
+        host_residual.assign(n, 1.0);
+
+        if (prec == LBM_PREC_F64) CU((prepare_kernels<double, double>()));
+        else CU((prepare_kernels<float, float>()));
+
+        // initial state (initialiseFunctions, cpuLBM.cpp:846-875)
+        std::vector<double> r0(total_nodes, 1.0), u0(total_nodes, 0.0), v0(total_nodes, 0.0), T0(total_nodes, 1.0);
+        for (int k = 0; k < n; ++k) {
+            const HostSample &h = hs[k];
+            for (int y = 0; y < h.ny; ++y)
+                for (int x = 0; x < h.nx; ++x) {
+                    const size_t src = (size_t)y * h.nx + x;
+                    const long long dst = sp[k].node_off + (long long)y * sp[k].pitch + x;
+                    r0[dst] = h.rho0[src];
+                    u0[dst] = h.ux0[src];
+                    v0[dst] = h.uy0[src];
+                    T0[dst] = h.T0[src];
+                }
+        }
+        DevBuf<double> dr, du, dv, dT;
+        dr.upload(r0, stream);
+        du.upload(u0, stream);
+        dv.upload(v0, stream);
+        dT.upload(T0, stream);
+        if (prec == LBM_PREC_F64) CU(launch_init<double>(args<double>(0), dr.p, du.p, dv.p, dT.p, stream));
+        else CU(launch_init<float>(args<float>(0), dr.p, du.p, dv.p, dT.p, stream));
+        CU(cudaStreamSynchronize(stream));
+        // equilibrium failures during initialisation are not reported by the
+        // reference (hasFailed is reset by runOne, cpuLBM.cpp:2288)
+        CU(cudaMemsetAsync(status.p, 0, n * sizeof(int), stream));
+        CU(cudaStreamSynchronize(stream));
+    }
+
+    static int &m_dummy()
+    {
+        static thread_local int m;
+        return m;
+    }
+
+    template <class S, class C>
+    void enqueue_step_t(int want_res)
+    {
+        const KArgs<S> a = args<S>(want_res);
+        const int nt = (int)tiles_all.size(), nt3 = (int)tiles_rk3.size();
+        CU((launch_phase<S, C>(a, 0, d_tiles_all.p, nt, nullptr, 0, stream)));
+        CU((launch_phase<S, C>(a, 3, nullptr, 0, d_walls_all.p, (int)walls_all.size(), stream)));
+        CU((launch_phase<S, C>(a, 1, d_tiles_all.p, nt, nullptr, 0, stream)));
+        if (any_rk3) {
+            CU((launch_phase<S, C>(a, 4, nullptr, 0, d_walls_rk3.p, (int)walls_rk3.size(), stream)));
+            CU((launch_phase<S, C>(a, 2, d_tiles_rk3.p, nt3, nullptr, 0, stream)));
+        }
+        if (want_res)
+            CU(launch_residual(d_sp.p, (int)hs.size(), partial.p, d_tile_first.p, d_tile_count.p, residual.p, stream));
+    }
+
+    void enqueue_step(int want_res)
+    {
+        if (prec == LBM_PREC_F64) enqueue_step_t<double, double>(want_res);
+        else enqueue_step_t<float, float>(want_res);
+    }
+
+    void launch_steps(int n, int want_res)
+    {
+        const int g = want_res ? 1 : 0;
+        if (use_graph && !graph[g]) {
+            cudaGraph_t gr;
+            CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_step(want_res);
+            } catch (...) {
+                cudaStreamEndCapture(stream, &gr);
+                throw;
+            }
+            CU(cudaStreamEndCapture(stream, &gr));
+            CU(cudaGraphInstantiate(&graph[g], gr, 0));
+            cudaGraphDestroy(gr);
+        }
+        for (int k = 0; k < n; ++k) {
+            if (use_graph) CU(cudaGraphLaunch(graph[g], stream));
+            else enqueue_step(want_res);
+        }
+    }
+
+    // collect and clear the per-sample status words
+    void fetch_status()
+    {
+        std::vector<int> st(hs.size());
+        CU(cudaMemcpyAsync(st.data(), status.p, st.size() * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CU(cudaMemsetAsync(status.p, 0, st.size() * sizeof(int), stream));
+        CU(cudaStreamSynchronize(stream));
+        for (size_t k = 0; k < st.size(); ++k) host_status[k] |= st[k];
+    }
+
+    void fetch_residual()
+    {
+        CU(cudaMemcpyAsync(host_residual.data(), residual.p, host_residual.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+    }
+
+    static lbm_status to_status(int bits)
+    {
+        if (bits & STATUS_EQ) return LBM_ERR_EQUILIBRIUM;
+        if (bits & STATUS_NONFINITE) return LBM_ERR_NONFINITE;
+        return LBM_OK;
+    }
+
+    void get_macro(int s, double *rho, double *ux, double *uy, double *T, double *p)
+    {
+        const long long n = (long long)hs[s].nx * hs[s].ny;
+        if (prec == LBM_PREC_F64)
+            CU(launch_macro_out<double>(d_sp.p, s, reinterpret_cast<double *>(state.p), scratch.p, n, stream));
+        else
+            CU(launch_macro_out<float>(d_sp.p, s, reinterpret_cast<float *>(state.p), scratch.p, n, stream));
+        double *dst[5] = {rho, ux, uy, T, p};
+        for (int k = 0; k < 5; ++k)
+            if (dst[k]) CU(cudaMemcpyAsync(dst[k], scratch.p + k * n, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+    }
+
+    void dist_io(int s, double *f, double *h, const double *fin, const double *hin)
+    {
+        const long long n = (long long)hs[s].nx * hs[s].ny;
+        const long long n3 = n * NQ;
+        const bool to_aos = fin == nullptr;
+        if (!to_aos) {
+            CU(cudaMemcpyAsync(scratch.p, fin, n3 * sizeof(double), cudaMemcpyHostToDevice, stream));
+            CU(cudaMemcpyAsync(scratch.p + n3, hin, n3 * sizeof(double), cudaMemcpyHostToDevice, stream));
+        }
+        if (prec == LBM_PREC_F64)
+            CU(launch_dist_io<double>(d_sp.p, s, reinterpret_cast<double *>(state.p), reinterpret_cast<double *>(buf2.p),
+                                      reinterpret_cast<double *>(buf3.p), scratch.p, to_aos ? 1 : 0, nflags.p, n, stream));
+        else
+            CU(launch_dist_io<float>(d_sp.p, s, reinterpret_cast<float *>(state.p), reinterpret_cast<float *>(buf2.p),
+                                     reinterpret_cast<float *>(buf3.p), scratch.p, to_aos ? 1 : 0, nflags.p, n, stream));
+        if (to_aos) {
+            if (f) CU(cudaMemcpyAsync(f, scratch.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            if (h) CU(cudaMemcpyAsync(h, scratch.p + n3, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        }
+        CU(cudaStreamSynchronize(stream));
+    }
+
+    size_t device_bytes() const
+    {
+        return state.n + buf2.n + buf3.n + alpha.n + nflags.n + sizeof(double) * (told.n + partial.n + scratch.n);
+    }
+};
+
+struct lbm_handle {
+    lbm_batch b;
+};
+
+// ---------------------------------------------------------------- C ABI
+#define API_BEGIN try {
+#define API_END                                          \
+    }                                                    \
+    catch (const LbmError &e)                            \
+    {                                                    \
+        g_last_error = e.what();                         \
+        return e.code;                                   \
+    }                                                    \
+    catch (const std::bad_alloc &)                       \
+    {                                                    \
+        g_last_error = "host allocation failed";         \
+        return LBM_ERR_NOMEM;                            \
+    }                                                    \
+    catch (const std::exception &e)                      \
+    {                                                    \
+        g_last_error = e.what();                         \
+        return LBM_ERR_INVALID;                          \
+    }
+
+extern "C" {
+
+const char *lbm_last_error(void) { return g_last_error.c_str(); }
+
+lbm_status lbm_create(const lbm_config *cfg, const lbm_init *init, int precision, lbm_handle **out)
+{
+    API_BEGIN
+    if (!cfg || !init || !out) throw LbmError(LBM_ERR_INVALID, "null argument");
+    *out = nullptr;
+    std::unique_ptr<lbm_handle> h(new lbm_handle);
+    lbm_batch_options o{precision, 0, 0, 1};
+    h->b.build(1, cfg, init, &o);
+    *out = h.release();
+    return LBM_OK;
+    API_END
+}
+
+void lbm_destroy(lbm_handle *h) { delete h; }
+
+void *lbm_stream(lbm_handle *h) { return h ? (void *)h->b.stream : nullptr; }
+
+lbm_status lbm_step(lbm_handle *h, int n_steps, int want_residual, double *residual_out)
+{
+    API_BEGIN
+    if (!h || n_steps < 0) throw LbmError(LBM_ERR_INVALID, "bad argument");
+    lbm_batch &b = h->b;
+    HostSample &s = b.hs[0];
+    b.host_status[0] = 0;
+    if (want_residual) {
+        // the residual belongs to each step; step one at a time
+        for (int k = 0; k < n_steps; ++k) {
+            s.step += 1;
+            b.launch_steps(1, 1);
+            b.fetch_residual();
+            s.residual = b.host_residual[0];
+        }
+    } else {
+        b.launch_steps(n_steps, 0);
+        s.step += n_steps;
+    }
+    b.fetch_status();
+    if (residual_out) *residual_out = s.residual;
+    return lbm_batch::to_status(b.host_status[0]);
+    API_END
+}
+
+lbm_status lbm_run(lbm_handle *h, int max_steps, int *stop_out, double *trace, int trace_len)
+{
+    API_BEGIN
+    if (!h) throw LbmError(LBM_ERR_INVALID, "null handle");
+    lbm_batch &b = h->b;
+    HostSample &s = b.hs[0];
+    const int numRes = 20;
+    int stop = 0, k = 0;
+    lbm_status last = LBM_OK;
+    while (stop == 0 && (max_steps < 0 || k < max_steps)) {
+        s.step += 1;
+        b.host_status[0] = 0;
+        if (s.tol != 0) {
+            b.launch_steps(1, 1);
+            b.fetch_residual();
+            b.fetch_status();
+            s.residual = b.host_residual[0];
+            stop = (b.host_status[0] & STATUS_EQ) ? 1 : 0;
+            if (s.step >= 2 && s.step <= numRes) {
+                s.initRes[s.step - 2] = s.residual;
+                s.residual = 1;
+            } else if (s.step == numRes + 1) {
+                for (int i = 0; i < numRes - 1; ++i) s.resNorm = std::max(s.initRes[i], s.resNorm);
+                s.residual = s.residual / s.resNorm;
+            } else if (s.step >= numRes + 1) {
+                s.residual = s.residual / s.resNorm;
+            }
+        } else {
+            b.launch_steps(1, 0);
+            b.fetch_status();
+            stop = (b.host_status[0] & STATUS_EQ) ? 1 : 0;
+        }
+        if (b.host_status[0] & STATUS_NONFINITE) last = LBM_ERR_NONFINITE;
+        if (trace && k < trace_len) trace[k] = s.residual;
+        if (s.step >= s.nsteps && s.nsteps != 0) stop = 2;
+        if (s.tol != 0 && s.residual <= s.tol && s.step >= numRes + 1) stop = 2;
+        ++k;
+    }
+    if (stop_out) *stop_out = stop;
+    return stop == 1 ? LBM_ERR_EQUILIBRIUM : last;
+    API_END
+}
+
+lbm_status lbm_get_macro(lbm_handle *h, double *rho, double *ux, double *uy, double *T, double *p)
+{
+    API_BEGIN
+    if (!h) throw LbmError(LBM_ERR_INVALID, "null handle");
+    h->b.get_macro(0, rho, ux, uy, T, p);
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_get_dist(lbm_handle *h, double *f, double *hh)
+{
+    API_BEGIN
+    if (!h) throw LbmError(LBM_ERR_INVALID, "null handle");
+    h->b.dist_io(0, f, hh, nullptr, nullptr);
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_set_dist(lbm_handle *h, const double *f, const double *hh)
+{
+    API_BEGIN
+    if (!h || !f || !hh) throw LbmError(LBM_ERR_INVALID, "null argument");
+    h->b.dist_io(0, nullptr, nullptr, f, hh);
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_get_info(lbm_handle *h, lbm_info *info)
+{
+    API_BEGIN
+    if (!h || !info) throw LbmError(LBM_ERR_INVALID, "null argument");
+    const HostSample &s = h->b.hs[0];
+    info->Nx = s.nx;
+    info->Ny = s.ny;
+    info->step = s.step;
+    info->nsteps = s.nsteps;
+    info->dt = s.dt;
+    info->tstep = s.step * s.dt;
+    info->residual = s.residual;
+    info->precision = h->b.prec;
+    info->rkmethod = s.rk;
+    info->fmethod = s.fm;
+    info->device_bytes = h->b.device_bytes();
+    return LBM_OK;
+    API_END
+}
+
+// ---------------------------------------------------------------- batches
+lbm_status lbm_batch_create(int n, const lbm_config *cfgs, const lbm_init *inits, const lbm_batch_options *opt,
+                            lbm_batch **out)
+{
+    API_BEGIN
+    if (!out) throw LbmError(LBM_ERR_INVALID, "null argument");
+    *out = nullptr;
+    std::unique_ptr<lbm_batch> b(new lbm_batch);
+    b->build(n, cfgs, inits, opt);
+    *out = b.release();
+    return LBM_OK;
+    API_END
+}
+
+void lbm_batch_destroy(lbm_batch *b) { delete b; }
+
+void *lbm_batch_stream(lbm_batch *b) { return b ? (void *)b->stream : nullptr; }
+
+long long lbm_batch_nodes(lbm_batch *b) { return b ? b->lattice_nodes : 0; }
+
+lbm_status lbm_batch_step(lbm_batch *b, int n_steps, int want_residual)
+{
+    API_BEGIN
+    if (!b || n_steps < 0) throw LbmError(LBM_ERR_INVALID, "bad argument");
+    b->launch_steps(n_steps, want_residual ? 1 : 0);
+    for (auto &s : b->hs) s.step += n_steps;
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_batch_status(lbm_batch *b, int *status)
+{
+    API_BEGIN
+    if (!b || !status) throw LbmError(LBM_ERR_INVALID, "null argument");
+    b->fetch_status();
+    for (size_t k = 0; k < b->hs.size(); ++k) {
+        status[k] = (int)lbm_batch::to_status(b->host_status[k]);
+        b->host_status[k] = 0;
+    }
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_batch_residuals(lbm_batch *b, double *residual)
+{
+    API_BEGIN
+    if (!b || !residual) throw LbmError(LBM_ERR_INVALID, "null argument");
+    b->fetch_residual();
+    std::copy(b->host_residual.begin(), b->host_residual.end(), residual);
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_batch_get_macro(lbm_batch *b, int sample, double *rho, double *ux, double *uy, double *T, double *p)
+{
+    API_BEGIN
+    if (!b || sample < 0 || sample >= (int)b->hs.size()) throw LbmError(LBM_ERR_INVALID, "bad sample");
+    b->get_macro(sample, rho, ux, uy, T, p);
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_batch_get_dist(lbm_batch *b, int sample, double *f, double *hh)
+{
+    API_BEGIN
+    if (!b || sample < 0 || sample >= (int)b->hs.size()) throw LbmError(LBM_ERR_INVALID, "bad sample");
+    b->dist_io(sample, f, hh, nullptr, nullptr);
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_batch_set_dist(lbm_batch *b, int sample, const double *f, const double *hh)
+{
+    API_BEGIN
+    if (!b || !f || !hh || sample < 0 || sample >= (int)b->hs.size()) throw LbmError(LBM_ERR_INVALID, "bad argument");
+    b->dist_io(sample, nullptr, nullptr, f, hh);
+    return LBM_OK;
+    API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,64 @@
+// Host-visible kernel interface of the D2Q13 LBM step (see lbm_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace uqlbm {
+
+struct SampleParams;
+struct Tile;
+
+constexpr int STATUS_EQ = 1;         // equilibrium mass check (cpuLBM.cpp:839-843)
+constexpr int STATUS_NONFINITE = 2;  // NaN / Inf / rho <= 0 in the state
+
+struct WallNode {
+    int sample, x, y, pad;
+};
+
+// Everything a phase kernel needs, passed by value.
+template <class S>
+struct KArgs {
+    const SampleParams *samples;
+    const Tile *tiles;
+    int ntiles;
+    int tx, ty;  // tile shape (threads = tx * ty)
+    S *state;    // f, h (and, between P1 and P2 of RK3, the update partial sum)
+    S *buf2;     // stage buffer 2 (f1 or f2)
+    S *buf3;     // stage buffer 3 (f3)
+    const uint8_t *nflags;
+    void *alpha_raw;
+    double *told;     // T at the start of the step (residual)
+    double *partial;  // per-tile residual partial sums
+    int *status;      // per-sample status bits
+    const double *tdx, *tdy, *dxv, *dyv;
+    int want_residual;
+    double eq_tol;
+#ifdef __CUDACC__
+    // alpha is stored in the compute type of the kernel instantiation
+    template <class C>
+    __device__ __forceinline__ C *alpha_as() const { return reinterpret_cast<C *>(alpha_raw); }
+#endif
+};
+
+template <class S, class C>
+cudaError_t launch_phase(const KArgs<S> &a, int phase, const Tile *tiles, int ntiles, const WallNode *walls,
+                         int nwalls, cudaStream_t st);
+template <class S, class C>
+cudaError_t prepare_kernels();
+size_t flux_smem_bytes(int prec, int tx, int ty);
+template <class S>
+cudaError_t launch_init(const KArgs<S> &a, const double *rho, const double *ux, const double *uy, const double *T,
+                        cudaStream_t st);
+template <class S>
+cudaError_t launch_macro_out(const SampleParams *samples, int s, const S *state, double *out, long long nodes,
+                             cudaStream_t st);
+template <class S>
+cudaError_t launch_dist_io(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, double *aos, int to_aos,
+                           const uint8_t *nflags, long long nodes, cudaStream_t st);
+cudaError_t launch_residual(const SampleParams *samples, int nsamples, const double *partial, const int *tile_first,
+                            const int *tile_count, double *residual, cudaStream_t st);
+
+}  // namespace uqlbm

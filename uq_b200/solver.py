@@ -1,0 +1,236 @@
+"""Python host mirror of the reference's step API over the C ABI.
+
+``Solver`` mirrors the C++ class ``cpuLBM``
+(CODE/C++/VS2010/simLB/simLB/cpuLBM.h:16-175): it is built from a case (the
+MAT variables of ``loadInput``, see ``uq_b200.workloads``), steps with
+``runOne`` / ``run`` and exposes ``rho_G, u_G, T_G, p_G, f_G, h_G`` in the
+reference's layouts (``macros.h:8-14``).  ``Batch`` advances many samples
+in one launch sequence.  Both run only on the CUDA library; a missing
+library raises.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import native as N
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+class _CaseBuffers:
+    """Holds the numpy arrays a config/init struct points into."""
+
+    def __init__(self, case):
+        self.keep = []
+        cfg = N.LbmConfig()
+        for name, _ in N.LbmConfig._fields_:
+            if name in ("dx_array", "dy_array"):
+                continue
+            setattr(cfg, name, type(getattr(cfg, name))(case.get(name, 0)))
+        for name in ("dx_array", "dy_array"):
+            if case.get(name) is not None:
+                arr = np.ascontiguousarray(case[name], dtype=np.float64)
+                self.keep.append(arr)
+                setattr(cfg, name, _d(arr))
+        bnd = np.ascontiguousarray(case["bnd"], dtype=np.int32)
+        ini = N.LbmInit()
+        ini.Nx, ini.Ny = bnd.shape
+        ini.numProps = int(case["numProps"])
+        arrs = dict(bndArray=bnd.reshape(-1), cellType=np.ascontiguousarray(case["cellType"], dtype=np.int32))
+        for k in ("density", "pressure", "temp", "velocityX", "velocityY"):
+            arrs[k] = np.ascontiguousarray(case[k], dtype=np.float64)
+        for k, a in arrs.items():
+            self.keep.append(a)
+            setattr(ini, k, a.ctypes.data_as(_ip if a.dtype == np.int32 else _dp))
+        self.cfg, self.ini = cfg, ini
+        self.nx, self.ny = bnd.shape
+
+
+class Solver:
+    """One solver instance (an ``lbm_handle``): the drop-in for cpuLBM."""
+
+    def __init__(self, case, precision="f64"):
+        L = N.lib()
+        self._bufs = _CaseBuffers(case)
+        self.nx, self.ny = self._bufs.nx, self._bufs.ny
+        h = C.c_void_p()
+        N.check(L.lbm_create(C.byref(self._bufs.cfg), C.byref(self._bufs.ini), N.PREC[precision], C.byref(h)),
+                "lbm_create")
+        self._h = h
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().lbm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- stepping (cpuLBM::updateStepCount + runOne; main.cpp runSimStep)
+    def runOne(self, res=0):
+        """One step; returns 1 where the reference's runOne returns hasFailed."""
+        code = N.lib().lbm_step(self._h, 1, 1 if res else 0, None)
+        if code not in (N.LBM_OK, N.LBM_ERR_EQUILIBRIUM, N.LBM_ERR_NONFINITE):
+            N.check(code, "lbm_step")
+        return 1 if code == N.LBM_ERR_EQUILIBRIUM else 0
+
+    def step(self, n=1, residual=False):
+        """n steps; returns (lbm_status, residual)."""
+        r = C.c_double(0)
+        code = N.lib().lbm_step(self._h, int(n), 1 if residual else 0, C.byref(r))
+        if code not in (N.LBM_OK, N.LBM_ERR_EQUILIBRIUM, N.LBM_ERR_NONFINITE):
+            N.check(code, "lbm_step")
+        return code, r.value
+
+    def run(self, max_steps=-1, trace_len=None):
+        """The reference driver loop; returns (stop, residual trace)."""
+        if trace_len is None:
+            trace_len = max_steps if max_steps >= 0 else max(self.info().nsteps, 1)
+        trace = np.zeros(max(int(trace_len), 1))
+        stop = C.c_int(0)
+        code = N.lib().lbm_run(self._h, int(max_steps), C.byref(stop), _d(trace), int(trace_len))
+        if code not in (N.LBM_OK, N.LBM_ERR_EQUILIBRIUM, N.LBM_ERR_NONFINITE):
+            N.check(code, "lbm_run")
+        return stop.value, trace
+
+    # -- state
+    def info(self):
+        inf = N.LbmInfo()
+        N.check(N.lib().lbm_get_info(self._h, C.byref(inf)), "lbm_get_info")
+        return inf
+
+    @property
+    def dt(self):
+        return self.info().dt
+
+    @property
+    def nsteps(self):
+        return self.info().nsteps
+
+    @property
+    def step_count(self):
+        return self.info().step
+
+    def macro(self):
+        n = self.nx * self.ny
+        out = {k: np.empty(n) for k in ("rho", "ux", "uy", "T", "p")}
+        N.check(N.lib().lbm_get_macro(self._h, *[_d(out[k]) for k in ("rho", "ux", "uy", "T", "p")]),
+                "lbm_get_macro")
+        return {k: v.reshape(self.nx, self.ny) for k, v in out.items()}
+
+    def dist(self):
+        n = self.nx * self.ny * 13
+        f, h = np.empty(n), np.empty(n)
+        N.check(N.lib().lbm_get_dist(self._h, _d(f), _d(h)), "lbm_get_dist")
+        return f.reshape(self.nx, self.ny, 13), h.reshape(self.nx, self.ny, 13)
+
+    def set_dist(self, f, h):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        N.check(N.lib().lbm_set_dist(self._h, _d(f), _d(h)), "lbm_set_dist")
+
+    @property
+    def rho_G(self):
+        return self.macro()["rho"]
+
+    @property
+    def T_G(self):
+        return self.macro()["T"]
+
+    @property
+    def p_G(self):
+        return self.macro()["p"]
+
+    @property
+    def u_G(self):
+        m = self.macro()
+        return np.stack([m["ux"], m["uy"]], axis=-1)
+
+    @property
+    def f_G(self):
+        return self.dist()[0]
+
+    @property
+    def h_G(self):
+        return self.dist()[1]
+
+    @property
+    def stream(self):
+        return N.lib().lbm_stream(self._h)
+
+
+class Batch:
+    """Many samples advanced together (an ``lbm_batch``)."""
+
+    def __init__(self, cases, precision="f32", tile=(0, 0), use_graph=True):
+        L = N.lib()
+        self._bufs = [_CaseBuffers(c) for c in cases]
+        n = len(cases)
+        cfgs = (N.LbmConfig * n)(*[b.cfg for b in self._bufs])
+        inis = (N.LbmInit * n)(*[b.ini for b in self._bufs])
+        opt = N.LbmBatchOptions(N.PREC[precision], int(tile[0]), int(tile[1]), 1 if use_graph else 0)
+        h = C.c_void_p()
+        N.check(L.lbm_batch_create(n, cfgs, inis, C.byref(opt), C.byref(h)), "lbm_batch_create")
+        self._h = h
+        self.n = n
+        self.shapes = [(b.nx, b.ny) for b in self._bufs]
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().lbm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nodes(self):
+        return N.lib().lbm_batch_nodes(self._h)
+
+    @property
+    def stream(self):
+        return N.lib().lbm_batch_stream(self._h)
+
+    def step(self, n=1, residual=False):
+        N.check(N.lib().lbm_batch_step(self._h, int(n), 1 if residual else 0), "lbm_batch_step")
+
+    def status(self):
+        st = np.zeros(self.n, dtype=np.int32)
+        N.check(N.lib().lbm_batch_status(self._h, st.ctypes.data_as(_ip)), "lbm_batch_status")
+        return st
+
+    def residuals(self):
+        r = np.zeros(self.n)
+        N.check(N.lib().lbm_batch_residuals(self._h, _d(r)), "lbm_batch_residuals")
+        return r
+
+    def macro(self, s):
+        nx, ny = self.shapes[s]
+        out = {k: np.empty(nx * ny) for k in ("rho", "ux", "uy", "T", "p")}
+        N.check(N.lib().lbm_batch_get_macro(self._h, int(s), *[_d(out[k]) for k in ("rho", "ux", "uy", "T", "p")]),
+                "lbm_batch_get_macro")
+        return {k: v.reshape(nx, ny) for k, v in out.items()}
+
+    def dist(self, s):
+        nx, ny = self.shapes[s]
+        f, h = np.empty(nx * ny * 13), np.empty(nx * ny * 13)
+        N.check(N.lib().lbm_batch_get_dist(self._h, int(s), _d(f), _d(h)), "lbm_batch_get_dist")
+        return f.reshape(nx, ny, 13), h.reshape(nx, ny, 13)
+
+    def set_dist(self, s, f, h):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        N.check(N.lib().lbm_batch_set_dist(self._h, int(s), _d(f), _d(h)), "lbm_batch_set_dist")

@@ -83,11 +83,14 @@ RIEMANN_QUADRANTS = dict(
 )
 
 
-def riemann(nx=2048, ny=2048, tau=1e-3, steps=500, fmethod=0, rkmethod=0, Tc_Tref=1.0, CFL=0.5):
+def riemann(nx=2048, ny=2048, tau=1e-3, steps=500, fmethod=0, rkmethod=0, Tc_Tref=1.5, CFL=0.2):
     """Four-quadrant Riemann problem, transmissive (clamped) boundaries.
 
     Non-dimensional: R = 1, p_ref = 1, T = p / rho; mu = tau * p_ref.
-    Quadrant placement follows ``makeLaxLiu3.py:79-89``.
+    Quadrant placement follows ``makeLaxLiu3.py:79-89``; CFL 0.2 is the
+    reference setup's own (``makeLaxLiu3.py:22``).  Tc_Tref = 1.5 keeps the
+    D2Q13 equilibria positive for the coldest quadrant (T = 0.21): at
+    Tc_Tref = 1 the scheme diverges within a few hundred steps.
     """
     q = RIEMANN_QUADRANTS
     case = dict(BASE, mu=tau * 1.0, steps=steps, FMETHOD=fmethod, RKMETHOD=rkmethod,
@@ -151,6 +154,50 @@ def uq_ensemble(n=512, seed=1234, sides=(64, 128, 256, 512), steps=1000):
         samples.append(dict(u_w=u_w, tau=tau, Pr=Pr, nx=side, ny=side, steps=steps,
                             seed=seed * 100003 + k))
     return samples
+
+
+def random_state(nx, ny, seed, bc="transmissive", fmethod=1, rkmethod=1, solid_frac=0.0, steps=1,
+                 mu=0.05, Pr=0.71, du=0.1, drho=0.1, dT=0.1):
+    """Seeded random near-equilibrium state: every node is its own property
+    with rho in 1 +- drho, T in 1 +- dT, u in +-du; optionally a random
+    fraction of solid (cellType 2, at rest) and half as many permanent
+    (cellType 1) nodes.  ``bc`` is transmissive (clamped), periodic, mirror
+    (all four sides) or mixed (periodic x, mirror north)."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny
+    case = dict(BASE, steps=steps, FMETHOD=fmethod, RKMETHOD=rkmethod, mu=mu, Pr=Pr)
+    if bc == "periodic":
+        case.update(periodicX=1, periodicY=1)
+    elif bc == "mirror":
+        case.update(mirrorNorth=1, mirrorSouth=1, mirrorEast=1, mirrorWest=1)
+    elif bc == "mixed":
+        case.update(periodicX=1, mirrorNorth=1)
+    elif bc != "transmissive":
+        raise ValueError(bc)
+    rho = rng.uniform(1 - drho, 1 + drho, n)
+    T = rng.uniform(1 - dT, 1 + dT, n)
+    ux = rng.uniform(-du, du, n)
+    uy = rng.uniform(-du, du, n)
+    ct = np.zeros(n, dtype=np.int64)
+    if solid_frac > 0:
+        ct[rng.uniform(size=n) < solid_frac] = 2
+        ct[rng.uniform(size=n) < solid_frac / 2] = 1
+        ux[ct == 2] = 0.0
+        uy[ct == 2] = 0.0
+    props = dict(density=rho, pressure=np.zeros(n), temp=T, velocityX=ux, velocityY=uy, cellType=ct)
+    return _finish(case, props, np.arange(n).reshape(nx, ny))
+
+
+BUILDERS = dict(couette=couette, riemann=riemann, flat_plate=flat_plate, random_state=random_state)
+
+
+def build(name, overrides=None, **kwargs):
+    """Build a case by builder name, then apply ``overrides`` (extra or
+    replaced configuration variables); used by the golden fixtures."""
+    case = BUILDERS[name](**kwargs)
+    if overrides:
+        case.update(overrides)
+    return case
 
 
 def ensemble_case(sample):
