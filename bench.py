@@ -1,0 +1,385 @@
+"""Benchmark: batched D2Q13 thermal LBM throughput (f+h MLUPS) on B200.
+
+Workload (default): the UQ ensemble -- 512 Couette samples, square sides
+drawn from {64,128,256,512}, u_w~U(0.05,0.2), tau~U(0.02,0.1),
+Pr~U(0.6,1.0), WENO5 fluxes, RK3 (the reference's RKMETHOD 1), FP32 state
+with FP64 moment sums.  One bench step = one time step of every sample
+(1 LU = one node, f and h, all 13 velocities, all RK stages).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  Under torchrun each rank advances its own
+ensemble (weak scaling, no data-path collective); timings are the max over
+ranks.  ``--impl reference`` times the reference C++ solver (oracle/_ref,
+built from the reference's unmodified sources) on the host cores instead.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B_ALG_F32 = 208  # algorithmic bytes per LU: f and h (26 values) read + written once, 4-byte state
+B_ALG_F64 = 416
+WORKLOAD = "uq_ensemble_couette_weno5_rk3"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--samples", type=int, default=512)
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile", default="0,0")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fp:
+            d = json.load(fp)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as fp:
+            for line in fp:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_arm(n_procs, steps_per_proc, samples, seed_offset=0):
+    """Time the reference C++ solver (or, if it is absent, the FP64 C
+    restatement) on independent ensemble samples, one process per core."""
+    from oracle import refrun
+    from uq_b200 import workloads as W
+
+    picks = [d for d in samples if d["nx"] == 64][: max(n_procs, 1)]
+    while len(picks) < n_procs:
+        picks.append(dict(picks[-1], seed=picks[-1]["seed"] + 1))
+    lu = 0
+    if refrun.available():
+        kind = "reference"
+        tmp = tempfile.mkdtemp(prefix="refarm_")
+        procs = []
+        for k, d in enumerate(picks):
+            wd = os.path.join(tmp, "p%d" % k)
+            os.makedirs(wd)
+            case = W.ensemble_case(dict(d, steps=steps_per_proc))
+            refrun.write_lbmv(os.path.join(wd, "case.lbmv"), refrun.case_to_vars(case))
+            lu += case["bnd"].size * steps_per_proc
+        t0 = time.perf_counter()
+        for k in range(len(picks)):
+            wd = os.path.join(tmp, "p%d" % k)
+            procs.append(subprocess.Popen([refrun.REF_BIN, "case.lbmv", "out.lbmv", str(steps_per_proc)], cwd=wd,
+                                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+        for p in procs:
+            p.wait()
+        wall = time.perf_counter() - t0
+        subprocess.run(["rm", "-rf", tmp])
+    else:
+        kind = "port"
+        from oracle import oracle as O
+
+        case = W.ensemble_case(dict(picks[0], steps=steps_per_proc))
+        o = O.Oracle(case)
+        t0 = time.perf_counter()
+        o.step(steps_per_proc)
+        wall = time.perf_counter() - t0
+        lu = case["bnd"].size * steps_per_proc
+        n_procs = 1
+    return lu / wall / 1e6, n_procs, kind, wall
+
+
+def run_reference_impl(args, rank, world):
+    if rank != 0:
+        return
+    from uq_b200 import workloads as W
+
+    samples = W.uq_ensemble(n=args.samples, seed=args.seed)
+    ncores = os.cpu_count() or 1
+    per = 20
+    for _ in range(args.warmup):
+        cpu_reference_arm(ncores, 2, samples)
+    vals, walls = [], []
+    kind = "reference"
+    for _ in range(args.steps):
+        v, cores, kind, wall = cpu_reference_arm(ncores, per, samples)
+        vals.append(v)
+        walls.append(wall)
+    value = float(np.mean(vals))
+    out = {
+        "metric": "batched f+h MLUPS (UQ ensemble, WENO5 RK3)", "value": value, "unit": "MLUPS",
+        "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * float(np.mean(walls)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "samples": args.samples, "reference_sample":
+                   "%d independent reference processes, each one 64x64 ensemble sample for %d steps" % (ncores, per)},
+        "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": ncores, "kind": kind,
+                         "sample": "%d processes x 64x64 Couette sample x %d steps per bench step" % (ncores, per)},
+        "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def accuracy_probe(samples, steps=10):
+    """Mixed path vs the FP64 plain path on a few small samples after
+    `steps` steps: max relative L2 of rho, |u|, T."""
+    from uq_b200 import workloads as W
+    from uq_b200.solver import Batch
+
+    small = [d for d in samples if d["nx"] <= 128][:8]
+    cases = [W.ensemble_case(d) for d in small]
+    b32 = Batch(cases, "f32")
+    b64 = Batch(cases, "f64")
+    b32.step(steps)
+    b64.step(steps)
+    worst = {"rho": 0.0, "u": 0.0, "T": 0.0}
+    for k in range(len(cases)):
+        m, r = b32.macro(k), b64.macro(k)
+        worst["rho"] = max(worst["rho"], np.linalg.norm(m["rho"] - r["rho"]) / np.linalg.norm(r["rho"]))
+        worst["T"] = max(worst["T"], np.linalg.norm(m["T"] - r["T"]) / np.linalg.norm(r["T"]))
+        du = np.sqrt((m["ux"] - r["ux"]) ** 2 + (m["uy"] - r["uy"]) ** 2)
+        worst["u"] = max(worst["u"], np.linalg.norm(du) / np.linalg.norm(np.hypot(r["ux"], r["uy"])))
+    b32.close()
+    b64.close()
+    return {"steps": steps, "samples": len(cases), "l2_rel_max": worst}
+
+
+def plain_fp64_probe(samples, steps=10, n=32):
+    """The plain FP64 path (one handle per sample, as a drop-in for runOne)
+    on the first n samples: MLUPS, to compare with the batched path."""
+    import torch
+
+    from uq_b200 import workloads as W
+    from uq_b200.solver import Solver
+
+    picked = samples[:n]
+    solvers = [Solver(W.ensemble_case(d), "f64") for d in picked]
+    for s in solvers:
+        s.step(2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in solvers:
+        s.step(steps)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    lu = sum(d["nx"] * d["ny"] for d in picked) * steps
+    for s in solvers:
+        s.close()
+    return lu / wall / 1e6
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from uq_b200 import workloads as W
+    from uq_b200.solver import Batch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    samples = W.uq_ensemble(n=args.samples, seed=args.seed + 7919 * rank)
+    cases = [W.ensemble_case(d) for d in samples]
+    tx, ty = (int(v) for v in args.tile.split(","))
+    b = Batch(cases, precision=args.precision, tile=(tx, ty))
+    nodes = b.nodes
+    st = torch.cuda.ExternalStream(b.stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    b.step(args.warmup)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    b.step(args.steps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    ms_per_step = ms / args.steps
+    status = b.status()
+    value = nodes * world * args.steps / (ms * 1e3)
+
+    # per-phase device time (CUDA events on the batch's stream, no graph)
+    phases = b.profile(3)
+    names = ["pointwise", "walls2", "stencil1", "walls3", "stencil2", "residual"]
+    dom = int(np.argmax(phases[:5]))
+    peak, peak_kind = measured_peaks()
+    b_alg = B_ALG_F32 if args.precision == "f32" else B_ALG_F64
+    achieved = b_alg * nodes / (phases[dom] * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic_per_node.json")
+    if os.path.exists(tp):
+        with open(tp) as fp:
+            tb = json.load(fp).get("%s_%s" % (args.precision, names[dom]))
+        if tb:
+            traffic = float(tb) * nodes
+
+    # end to end through the C ABI: pinned host fields in, K steps, macros out
+    n_s = len(cases)
+    host_in, host_out = [], []
+    for k, c in enumerate(cases):
+        nn = c["bnd"].size
+        hi = torch.empty((4, nn), dtype=torch.float64, pin_memory=True)
+        ids = c["bnd"].reshape(-1)
+        hi[0] = torch.from_numpy(c["density"][ids])
+        hi[1] = torch.from_numpy(c["velocityX"][ids])
+        hi[2] = torch.from_numpy(c["velocityY"][ids])
+        hi[3] = torch.from_numpy(c["temp"][ids])
+        host_in.append(hi)
+        host_out.append(torch.empty((5, nn), dtype=torch.float64, pin_memory=True))
+    h2d = sum(h.numel() * 8 for h in host_in)
+    d2h = sum(h.numel() * 8 for h in host_out)
+    barrier()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(st)
+    for k in range(n_s):
+        hi = host_in[k]
+        b.set_macro_ptr(k, hi[0].data_ptr(), hi[1].data_ptr(), hi[2].data_ptr(), hi[3].data_ptr())
+    b.step(args.steps)
+    for k in range(n_s):
+        ho = host_out[k]
+        b.macro_ptr(k, *[ho[j].data_ptr() for j in range(5)])
+    e3.record(st)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e2.elapsed_time(e3))
+    e2e_value = nodes * world * args.steps / (e2e_ms * 1e3)
+
+    extra = {}
+    if rank == 0:
+        extra["accuracy_vs_fp64"] = accuracy_probe(samples)
+        try:
+            extra["plain_fp64_mlups_32_samples"] = plain_fp64_probe(samples)
+        except Exception as exc:  # reported, not fatal
+            extra["plain_fp64_mlups_32_samples"] = "error: %s" % exc
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, kind, wall = cpu_reference_arm(os.cpu_count() or 1, 20, samples)
+        cpu = {"value": v, "unit": "MLUPS", "cores": cores, "kind": kind,
+               "sample": "%d processes, each one 64x64 ensemble sample x 20 steps (%.1f s wall)" % (cores, wall)}
+
+    if rank == 0:
+        out = {
+            "metric": "batched f+h MLUPS (UQ ensemble, WENO5 RK3)", "value": value, "unit": "MLUPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "f32" else "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "samples_per_gpu": n_s, "sides": [64, 128, 256, 512],
+                       "nodes_per_step_per_gpu": nodes, "steps_per_solve": 1000,
+                       "precision": "FP32 state/stencils/collision, FP64 moment sums" if args.precision == "f32"
+                       else "FP64", "l2": "inputs larger than L2 (whole-ensemble state ~%.1f GB)" %
+                       (nodes * 26 * 4 * (4 if args.precision == "f32" else 8) / 1e9),
+                       "parallelism": "samples sharded per rank (dp%d)" % world, "seed": args.seed},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": "k_flux " + names[dom],
+                         "peak_kind": peak_kind, "alg_bytes_per_lu": b_alg,
+                         "phase_ms": dict(zip(names, [float(x) for x in phases]))},
+            "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d / args.steps,
+                    "d2h_bytes_per_step": d2h / args.steps,
+                    "what": "per solve: pinned host fields -> lbm_batch_set_macro, K steps, lbm_batch_get_macro"},
+            "gpu_launches": b.launches_per_step(False) * args.steps,
+            "clocks": clk,
+            "sample_status": {"ok": int((status == 0).sum()), "failed": int((status != 0).sum())},
+            "cpu_baseline": cpu,
+        }
+        out.update(extra)
+        print(json.dumps(out), flush=True)
+    b.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference_impl(args, rank, world)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

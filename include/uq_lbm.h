@@ -160,6 +160,18 @@ LBM_API lbm_status lbm_batch_get_macro(lbm_batch *b, int sample, double *rho, do
                                double *T, double *p);
 LBM_API lbm_status lbm_batch_get_dist(lbm_batch *b, int sample, double *f, double *hh);
 LBM_API lbm_status lbm_batch_set_dist(lbm_batch *b, int sample, const double *f, const double *hh);
+/* Set a sample's f, h to the equilibria of the given macroscopic fields
+ * (each [x*Ny + y]), as initialiseFunctions does for property tables
+ * (cpuLBM.cpp:846-875): the restart-from-fields / new-solve entry point. */
+LBM_API lbm_status lbm_batch_set_macro(lbm_batch *b, int sample, const double *rho, const double *ux,
+                                       const double *uy, const double *T);
+/* Run n_steps steps outside any graph with CUDA events around every phase
+ * and return the mean device milliseconds per step of each phase in
+ * phase_ms[0..5]: pointwise stages, walls of buffer 2, stencil phase 1,
+ * walls of buffer 3, stencil phase 2, residual reduction. */
+LBM_API lbm_status lbm_batch_profile(lbm_batch *b, int n_steps, double *phase_ms, int n_phases);
+/* Kernel launches one step of the batch issues. */
+LBM_API int lbm_batch_launches_per_step(lbm_batch *b, int want_residual);
 /* Lattice updates (nodes) one step of the whole batch performs. */
 LBM_API long long lbm_batch_nodes(lbm_batch *b);
 LBM_API void *lbm_batch_stream(lbm_batch *b);

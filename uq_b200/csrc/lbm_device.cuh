@@ -21,8 +21,10 @@ constexpr int NPL = 26;  // f and h planes
 constexpr uint8_t NF_TYPE = 3;
 constexpr uint8_t NF_SOLX = 4;
 constexpr uint8_t NF_SOLY = 8;
-constexpr uint8_t NF_EDGX = 16;
+constexpr uint8_t NF_EDGX = 16;   // near a clamped/mirrored x edge
 constexpr uint8_t NF_EDGY = 32;
+constexpr uint8_t NF_WRPX = 64;   // x stencil wraps across a periodic edge
+constexpr uint8_t NF_WRPY = 128;
 
 // sample flag bits
 constexpr int SF_PERX = 1, SF_PERY = 2, SF_MIRN = 4, SF_MIRS = 8, SF_MIRE = 16, SF_MIRW = 32;
@@ -51,6 +53,10 @@ __constant__ int c_EX[NQ] = {0, 1, 0, -1, 0, 1, -1, -1, 1, 2, 0, -2, 0};
 __constant__ int c_EY[NQ] = {0, 0, 1, 0, -1, 1, 1, -1, -1, 0, 2, 0, -2};
 __constant__ int c_MIR_NS[NQ] = {0, 1, 4, 3, 2, 8, 7, 6, 5, 9, 12, 11, 10};
 __constant__ int c_MIR_EW[NQ] = {0, 3, 2, 1, 4, 6, 5, 8, 7, 11, 10, 9, 12};
+
+// the same lattice as compile-time constants (for unrolled direction loops)
+constexpr int kEX[NQ] = {0, 1, 0, -1, 0, 1, -1, -1, 1, 2, 0, -2, 0};
+constexpr int kEY[NQ] = {0, 0, 1, 0, -1, 1, 1, -1, -1, 0, 2, 0, -2};
 
 __device__ __forceinline__ int isgn(int a) { return (a > 0) - (a < 0); }
 
@@ -223,15 +229,12 @@ __device__ __forceinline__ int bc_index(const SampleParams &sp, int i, int pm, i
 }
 
 // -------------------------------------------------------------- NND, WENO5
-// minmod with the reference's case order (cpuLBM.cpp:1130-1145)
+// minmod with the reference's case order (cpuLBM.cpp:1130-1145): same
+// signs -> the smaller magnitude (equal magnitudes mean a == b), else 0
 template <class C>
 __device__ __forceinline__ C minmod(C a, C b)
 {
-    C out = C(0);
-    if (fabs(a) < fabs(b) && a * b > C(0)) out = a;
-    else if (fabs(b) < fabs(a) && a * b > C(0)) out = b;
-    else if (a == b) out = a;
-    return out;
+    return a * b > C(0) ? (fabs(a) < fabs(b) ? a : b) : C(0);
 }
 
 // NND (cpuLBM.cpp:1328-1356) on the 3 upwind-ordered values s0, s1, s2
@@ -242,39 +245,46 @@ __device__ __forceinline__ C nnd3(C ae, C s0, C s1, C s2)
     return c + C(0.5) * minmod<C>(ae * s2 - c, c - ae * s0);
 }
 
-// WENO5 (cpuLBM.cpp:1358-1403): Jiang-Shu indicators, linear weights
+// one division per face (the FP64 path keeps it correctly rounded)
+__device__ __forceinline__ double face_div(double n, double d) { return n / d; }
+__device__ __forceinline__ float face_div(float n, float d) { return __fdividef(n, d); }
+
+// WENO5 (cpuLBM.cpp:1358-1403): Jiang-Shu indicators b_k, linear weights
 // 1/10, 6/10, 3/10, epsilon 1e-6, on |e| times the upwind-ordered values.
+// The nonlinear weights d_k/(eps+b_k)^2 normalised by their sum are formed
+// as d_k prod_{j!=k} (eps+b_j)^2 over the same sum, one division per face.
 template <class C>
 __device__ __forceinline__ C weno5(C ae, C s0, C s1, C s2, C s3, C s4)
 {
     const C q0 = ae * s0, q1 = ae * s1, q2 = ae * s2, q3 = ae * s3, q4 = ae * s4;
     const C d0 = q0 - C(2) * q1 + q2, d1 = q1 - C(2) * q2 + q3, d2 = q2 - C(2) * q3 + q4;
     const C l0 = q0 - C(4) * q1 + C(3) * q2, l1 = q1 - q3, l2 = C(3) * q2 - C(4) * q3 + q4;
-    const C b0 = C(13.0 / 12.0) * d0 * d0 + C(0.25) * l0 * l0;
-    const C b1 = C(13.0 / 12.0) * d1 * d1 + C(0.25) * l1 * l1;
-    const C b2 = C(13.0 / 12.0) * d2 * d2 + C(0.25) * l2 * l2;
-    const C g0 = C(1) / (C(1e-6) + b0), g1 = C(1) / (C(1e-6) + b1), g2 = C(1) / (C(1e-6) + b2);
-    const C w0 = C(0.1) * g0 * g0, w1 = C(0.6) * g1 * g1, w2 = C(0.3) * g2 * g2;
-    const C ws = w0 + w1 + w2;
-    const C r0 = (C(2) * q0 - C(7) * q1 + C(11) * q2) * C(1.0 / 6.0);
-    const C r1 = (-q1 + C(5) * q2 + C(2) * q3) * C(1.0 / 6.0);
-    const C r2 = (C(2) * q2 + C(5) * q3 - q4) * C(1.0 / 6.0);
-    return (w0 * r0 + w1 * r1 + w2 * r2) / ws;
+    const C a0 = C(1e-6) + (C(13.0 / 12.0) * d0 * d0 + C(0.25) * l0 * l0);
+    const C a1 = C(1e-6) + (C(13.0 / 12.0) * d1 * d1 + C(0.25) * l1 * l1);
+    const C a2 = C(1e-6) + (C(13.0 / 12.0) * d2 * d2 + C(0.25) * l2 * l2);
+    const C p0 = a0 * a0, p1 = a1 * a1, p2 = a2 * a2;
+    const C w0 = C(0.1) * (p1 * p2), w1 = C(0.6) * (p0 * p2), w2 = C(0.3) * (p0 * p1);
+    const C r0 = (C(2) * q0 - C(7) * q1 + C(11) * q2);
+    const C r1 = (-q1 + C(5) * q2 + C(2) * q3);
+    const C r2 = (C(2) * q2 + C(5) * q3 - q4);
+    return face_div(w0 * r0 + w1 * r1 + w2 * r2, C(6) * (w0 + w1 + w2));
 }
 
 // view of one sample's stage buffer and node flags
+// One sample's stage buffer and node flags; offsets inside a sample fit in
+// 32 bits (26 planes of up to 2^26 nodes).
 template <class S>
 struct StageView {
     const S *__restrict__ st;        // plane 0 of the sample in the stage buffer
     const uint8_t *__restrict__ nf;  // node flags of the sample
-    long long plane;
+    int plane;
     int pitch;
 };
 
 template <class S>
 __device__ __forceinline__ S ldv(const StageView<S> &v, int p, int x, int y)
 {
-    return __ldg(v.st + (long long)p * v.plane + (long long)y * v.pitch + x);
+    return __ldg(v.st + (p * v.plane + y * v.pitch + x));
 }
 
 // Exact stencil + reconstruction (stencil, cpuLBM.cpp:1171-1326, then NND/
@@ -282,7 +292,7 @@ __device__ __forceinline__ S ldv(const StageView<S> &v, int p, int x, int y)
 // indices with reflections, and the linear extrapolation 2 f(m1) - f(m2)
 // over the first solid/fluid edge met by the stencil.
 template <class S, class C>
-__device__ C flux_exact(const SampleParams &sp, const StageView<S> &v, int x, int y, int p, int axis)
+__device__ __noinline__ C flux_exact(const SampleParams &sp, const StageView<S> &v, int x, int y, int p, int axis)
 {
     const int i = p < NQ ? p : p - NQ, pb = p - i;
     const int e = axis == 0 ? isgn(c_EX[i]) : isgn(c_EY[i]);
@@ -302,7 +312,7 @@ __device__ C flux_exact(const SampleParams &sp, const StageView<S> &v, int x, in
             const int pp = m ? pb + (axis == 0 ? c_MIR_EW[i] : c_MIR_NS[i]) : p;
             const int xr = axis == 0 ? r : x, yr = axis == 0 ? y : r;
             S5[j] = (C)ldv(v, pp, xr, yr);
-            sld[j] = (v.nf[(long long)yr * v.pitch + xr] & NF_TYPE) == 2;
+            sld[j] = (v.nf[yr * v.pitch + xr] & NF_TYPE) == 2;
             any |= sld[j];
         }
     }
@@ -327,6 +337,30 @@ __device__ C flux_exact(const SampleParams &sp, const StageView<S> &v, int x, in
     return nnd3<C>(ae, S5[0], S5[1], S5[2]);
 }
 
+// Stencil across a periodic edge with no solid in it: the five neighbours
+// with single periodic wrap, read from global memory.
+template <class S, class C>
+__device__ __forceinline__ C flux_wrap(const SampleParams &sp, const StageView<S> &v, int x, int y, int p, int axis)
+{
+    const int i = p < NQ ? p : p - NQ;
+    const int ev = axis == 0 ? c_EX[i] : c_EY[i];
+    if (ev == 0) return C(0);
+    const int e = ev > 0 ? 1 : -1;
+    const C ae = (C)(sp.c * (double)abs(ev));
+    const int N = axis == 0 ? sp.nx : sp.ny;
+    const int pos = axis == 0 ? x : y;
+    C q[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        int r = pos + e * (j - 2);
+        r += r < 0 ? N : 0;
+        r -= r >= N ? N : 0;
+        q[j] = axis == 0 ? (C)ldv(v, p, r, y) : (C)ldv(v, p, x, r);
+    }
+    if (sp.fm) return weno5<C>(ae, q[0], q[1], q[2], q[3], q[4]);
+    return nnd3<C>(ae, q[1], q[2], q[3]);
+}
+
 // Outgoing face flux of plane p along `axis` at a non-solid node; the fast
 // path (no solid, no domain edge within the stencil) reads the five
 // neighbours directly.
@@ -339,10 +373,11 @@ __device__ __forceinline__ C flux_axis(const SampleParams &sp, const StageView<S
     if (ev == 0) return C(0);
     const uint8_t slow = axis == 0 ? (NF_SOLX | NF_EDGX) : (NF_SOLY | NF_EDGY);
     if (nflag & slow) return flux_exact<S, C>(sp, v, x, y, p, axis);
+    if (nflag & (axis == 0 ? NF_WRPX : NF_WRPY)) return flux_wrap<S, C>(sp, v, x, y, p, axis);
     const int e = ev > 0 ? 1 : -1;
     const C ae = (C)(sp.c * (double)abs(ev));
-    const long long stride = axis == 0 ? (long long)e : (long long)e * v.pitch;
-    const S *c0 = v.st + (long long)p * v.plane + (long long)y * v.pitch + x;
+    const int stride = axis == 0 ? e : e * v.pitch;
+    const S *c0 = v.st + (p * v.plane + y * v.pitch + x);
     if (sp.fm) {
         return weno5<C>(ae, (C)__ldg(c0 - 2 * stride), (C)__ldg(c0 - stride), (C)__ldg(c0), (C)__ldg(c0 + stride),
                         (C)__ldg(c0 + 2 * stride));

@@ -11,6 +11,8 @@
 #include "lbm_kernels.h"
 #include "../../include/uq_lbm.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -191,6 +193,22 @@ static HostSample derive(const lbm_config &c, const lbm_init &in)
 
 static int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda needed).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        CU(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p)
+            throw LbmError(LBM_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
 }  // namespace uqlbm
 
 using namespace uqlbm;
@@ -204,6 +222,7 @@ struct lbm_batch {
     std::vector<HostSample> hs;
     std::vector<SampleParams> sp;
     std::vector<Tile> tiles_all, tiles_rk3;
+    std::vector<Tile> tiles_by_rk[4];
     std::vector<WallNode> walls_all, walls_rk3;
     std::vector<int> tile_first, tile_count;
     long long total_state = 0, total_nodes = 0, lattice_nodes = 0;
@@ -216,7 +235,9 @@ struct lbm_batch {
     DevBuf<int> status, d_tile_first, d_tile_count;
     DevBuf<SampleParams> d_sp;
     DevBuf<Tile> d_tiles_all, d_tiles_rk3;
+    DevBuf<Tile> d_tiles_by_rk[4];
     DevBuf<WallNode> d_walls_all, d_walls_rk3;
+    DevBuf<CUtensorMap> d_maps;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [want_residual]
     std::vector<int> host_status;
     std::vector<double> host_residual;
@@ -251,6 +272,7 @@ struct lbm_batch {
         a.tdy = tdy.p;
         a.dxv = dxv.p;
         a.dyv = dyv.p;
+        a.tmaps = d_maps.p;
         a.want_residual = want_res;
         a.eq_tol = 1e-6;
         return a;
@@ -263,8 +285,8 @@ struct lbm_batch {
         if (prec != LBM_PREC_F64 && prec != LBM_PREC_F32) throw LbmError(LBM_ERR_INVALID, "unknown precision");
         if (opt && opt->tile_x > 0) tx = opt->tile_x;
         if (opt && opt->tile_y > 0) ty = opt->tile_y;
-        if (tx * ty > 256 || tx < 1 || ty < 1 || tx * ty % 32 != 0)
-            throw LbmError(LBM_ERR_INVALID, "tile must hold a multiple of 32 and at most 256 nodes");
+        if (tx * ty > 256 || tx < 4 || ty < 1 || tx * ty % 32 != 0 || tx % 4 != 0)
+            throw LbmError(LBM_ERR_INVALID, "tile must hold a multiple of 32 and at most 256 nodes, width a multiple of 4");
         use_graph = opt ? opt->use_graph != 0 : true;
         hs.reserve(n);
         for (int k = 0; k < n; ++k) hs.push_back(derive(cfgs[k], inits[k]));
@@ -320,8 +342,8 @@ struct lbm_batch {
                         if (h.type[(size_t)y * h.nx + xr] == 2) fl |= NF_SOLX;
                         if (h.type[(size_t)yr * h.nx + x] == 2) fl |= NF_SOLY;
                     }
-                    if (x < 2 || x > h.nx - 3) fl |= NF_EDGX;
-                    if (y < 2 || y > h.ny - 3) fl |= NF_EDGY;
+                    if (x < 2 || x > h.nx - 3) fl |= (h.flags & SF_PERX) ? NF_WRPX : NF_EDGX;
+                    if (y < 2 || y > h.ny - 3) fl |= (h.flags & SF_PERY) ? NF_WRPY : NF_EDGY;
                     flags[p.node_off + (long long)y * p.pitch + x] = fl;
                 }
             // tiles
@@ -330,6 +352,7 @@ struct lbm_batch {
                 for (int x0 = 0; x0 < h.nx; x0 += tx) {
                     Tile t{k, x0, y0, (int)tiles_all.size()};
                     tiles_all.push_back(t);
+                    tiles_by_rk[h.rk].push_back(t);
                     if (h.rk == 1) tiles_rk3.push_back(t);
                 }
             p.ntile = (int)tiles_all.size() - p.first_tile;
@@ -378,6 +401,7 @@ struct lbm_batch {
         d_sp.upload(sp, stream);
         d_tiles_all.upload(tiles_all, stream);
         d_tiles_rk3.upload(tiles_rk3, stream);
+        for (int m = 0; m < 4; ++m) d_tiles_by_rk[m].upload(tiles_by_rk[m], stream);
         d_walls_all.upload(walls_all, stream);
         d_walls_rk3.upload(walls_rk3, stream);
         d_tile_first.upload(tile_first, stream);
@@ -386,6 +410,28 @@ struct lbm_batch {
         host_status.assign(n, 0);
         host_residual.assign(n, 1.0);
 
+        // TMA descriptors: per sample and stage buffer, the 26 planes as a 3D
+        // tensor (x, y, plane) with the staged halo box of the flux kernels
+        {
+            auto enc = tensor_map_encoder();
+            std::vector<CUtensorMap> maps(2 * n);
+            const size_t es = elem();
+            for (int k = 0; k < n; ++k)
+                for (int b = 0; b < 2; ++b) {
+                    unsigned char *base = (b == 0 ? buf2.p : buf3.p) + (size_t)sp[k].state_off * es;
+                    cuuint64_t dims[3] = {(cuuint64_t)sp[k].nx, (cuuint64_t)sp[k].ny, (cuuint64_t)NPL};
+                    cuuint64_t strides[2] = {(cuuint64_t)sp[k].pitch * es, (cuuint64_t)sp[k].plane * es};
+                    cuuint32_t box[3] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 6), 1};
+                    cuuint32_t estr[3] = {1, 1, 1};
+                    CUresult r = enc(&maps[2 * k + b],
+                                     prec == LBM_PREC_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                                     3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                    if (r != CUDA_SUCCESS) throw LbmError(LBM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+                }
+            d_maps.upload(maps, stream);
+        }
         if (prec == LBM_PREC_F64) CU((prepare_kernels<double, double>()));
         else CU((prepare_kernels<float, float>()));
 
@@ -423,20 +469,74 @@ struct lbm_batch {
         return m;
     }
 
+    // One step.  ev (optional) receives 7 events around the phases:
+    // [0] start, then after pointwise, walls 2, phase 1, walls 3, phase 2,
+    // residual.
     template <class S, class C>
-    void enqueue_step_t(int want_res)
+    void enqueue_step_t(int want_res, cudaEvent_t *ev = nullptr)
     {
         const KArgs<S> a = args<S>(want_res);
-        const int nt = (int)tiles_all.size(), nt3 = (int)tiles_rk3.size();
-        CU((launch_phase<S, C>(a, 0, d_tiles_all.p, nt, nullptr, 0, stream)));
-        CU((launch_phase<S, C>(a, 3, nullptr, 0, d_walls_all.p, (int)walls_all.size(), stream)));
-        CU((launch_phase<S, C>(a, 1, d_tiles_all.p, nt, nullptr, 0, stream)));
-        if (any_rk3) {
-            CU((launch_phase<S, C>(a, 4, nullptr, 0, d_walls_rk3.p, (int)walls_rk3.size(), stream)));
-            CU((launch_phase<S, C>(a, 2, d_tiles_rk3.p, nt3, nullptr, 0, stream)));
-        }
+        if (ev) CU(cudaEventRecord(ev[0], stream));
+        // pointwise stages, per method
+        for (int m = 0; m < 4; ++m)
+            if (!tiles_by_rk[m].empty())
+                CU((launch_phase<S, C>(a, 0, m, d_tiles_by_rk[m].p, (int)tiles_by_rk[m].size(), nullptr, 0, stream)));
+        if (ev) CU(cudaEventRecord(ev[1], stream));
+        CU((launch_phase<S, C>(a, 3, 0, nullptr, 0, d_walls_all.p, (int)walls_all.size(), stream)));
+        if (ev) CU(cudaEventRecord(ev[2], stream));
+        for (int m = 0; m < 4; ++m)
+            if (!tiles_by_rk[m].empty())
+                CU((launch_phase<S, C>(a, 1, m, d_tiles_by_rk[m].p, (int)tiles_by_rk[m].size(), nullptr, 0, stream)));
+        if (ev) CU(cudaEventRecord(ev[3], stream));
+        if (any_rk3) CU((launch_phase<S, C>(a, 4, 1, nullptr, 0, d_walls_rk3.p, (int)walls_rk3.size(), stream)));
+        if (ev) CU(cudaEventRecord(ev[4], stream));
+        if (any_rk3) CU((launch_phase<S, C>(a, 2, 1, d_tiles_rk3.p, (int)tiles_rk3.size(), nullptr, 0, stream)));
+        if (ev) CU(cudaEventRecord(ev[5], stream));
         if (want_res)
             CU(launch_residual(d_sp.p, (int)hs.size(), partial.p, d_tile_first.p, d_tile_count.p, residual.p, stream));
+        if (ev) CU(cudaEventRecord(ev[6], stream));
+    }
+
+    int launches_per_step(int want_res) const
+    {
+        int n = 0;
+        for (int m = 0; m < 4; ++m) n += tiles_by_rk[m].empty() ? 0 : 2;  // pointwise + stencil
+        n += walls_all.empty() ? 0 : 1;
+        if (any_rk3) n += (walls_rk3.empty() ? 0 : 1) + 1;
+        return n + (want_res ? 1 : 0);
+    }
+
+    void profile(int n, double *ms, int nph)
+    {
+        cudaEvent_t ev[7];
+        for (auto &e : ev) CU(cudaEventCreate(&e));
+        std::vector<double> acc(6, 0.0);
+        for (int k = 0; k < n; ++k) {
+            if (prec == LBM_PREC_F64) enqueue_step_t<double, double>(1, ev);
+            else enqueue_step_t<float, float>(1, ev);
+            CU(cudaEventSynchronize(ev[6]));
+            for (int p = 0; p < 6; ++p) {
+                float t = 0;
+                CU(cudaEventElapsedTime(&t, ev[p], ev[p + 1]));
+                acc[p] += t;
+            }
+        }
+        for (auto &e : ev) cudaEventDestroy(e);
+        for (int p = 0; p < nph && p < 6; ++p) ms[p] = n ? acc[p] / n : 0.0;
+    }
+
+    void set_macro(int s, const double *rho, const double *ux, const double *uy, const double *T)
+    {
+        const long long n = (long long)hs[s].nx * hs[s].ny;
+        const double *src[4] = {rho, ux, uy, T};
+        for (int k = 0; k < 4; ++k)
+            CU(cudaMemcpyAsync(scratch.p + k * n, src[k], n * sizeof(double), cudaMemcpyHostToDevice, stream));
+        if (prec == LBM_PREC_F64)
+            CU(launch_set_macro<double>(d_sp.p, s, reinterpret_cast<double *>(state.p), reinterpret_cast<double *>(buf2.p),
+                                        reinterpret_cast<double *>(buf3.p), scratch.p, nflags.p, n, stream));
+        else
+            CU(launch_set_macro<float>(d_sp.p, s, reinterpret_cast<float *>(state.p), reinterpret_cast<float *>(buf2.p),
+                                       reinterpret_cast<float *>(buf3.p), scratch.p, nflags.p, n, stream));
     }
 
     void enqueue_step(int want_res)
@@ -486,6 +586,7 @@ struct lbm_batch {
 
     static lbm_status to_status(int bits)
     {
+        if (bits & STATUS_TIMEOUT) return LBM_ERR_TIMEOUT;
         if (bits & STATUS_EQ) return LBM_ERR_EQUILIBRIUM;
         if (bits & STATUS_NONFINITE) return LBM_ERR_NONFINITE;
         return LBM_OK;
@@ -762,6 +863,29 @@ lbm_status lbm_batch_get_dist(lbm_batch *b, int sample, double *f, double *hh)
     return LBM_OK;
     API_END
 }
+
+lbm_status lbm_batch_set_macro(lbm_batch *b, int sample, const double *rho, const double *ux, const double *uy,
+                               const double *T)
+{
+    API_BEGIN
+    if (!b || !rho || !ux || !uy || !T || sample < 0 || sample >= (int)b->hs.size())
+        throw LbmError(LBM_ERR_INVALID, "bad argument");
+    b->set_macro(sample, rho, ux, uy, T);
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_batch_profile(lbm_batch *b, int n_steps, double *phase_ms, int n_phases)
+{
+    API_BEGIN
+    if (!b || !phase_ms || n_steps < 1) throw LbmError(LBM_ERR_INVALID, "bad argument");
+    b->profile(n_steps, phase_ms, n_phases);
+    for (auto &s : b->hs) s.step += n_steps;
+    return LBM_OK;
+    API_END
+}
+
+int lbm_batch_launches_per_step(lbm_batch *b, int want_residual) { return b ? b->launches_per_step(want_residual) : 0; }
 
 lbm_status lbm_batch_set_dist(lbm_batch *b, int sample, const double *f, const double *hh)
 {

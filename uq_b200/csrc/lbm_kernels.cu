@@ -14,6 +14,7 @@
 // (cpuLBM.cpp:1597-2283) with full-field temporaries.
 #include "lbm_device.cuh"
 #include "lbm_kernels.h"
+#include "tma.cuh"
 
 #include <cuda_runtime.h>
 
@@ -77,8 +78,9 @@ __device__ __forceinline__ Macro node_macro(const S *__restrict__ st, const Samp
 }
 
 // ------------------------------------------------------------------- P0
-template <class S, class C>
-__global__ void __launch_bounds__(256) k_stage0(KArgs<S> a)
+// RK: 1 (RK3 stages 1+2), 0 (RK1 stage 1), 2 (EULER / EULER_EQ: copy)
+template <class S, class C, int RK>
+__global__ void __launch_bounds__(256, 2) k_stage0(KArgs<S> a)
 {
     const Tile t = a.tiles[blockIdx.x];
     const SampleParams sp = a.samples[t.sample];
@@ -89,7 +91,7 @@ __global__ void __launch_bounds__(256) k_stage0(KArgs<S> a)
     const int type = a.nflags[node] & NF_TYPE;
     const S *st = a.state + sp.state_off;
     S *b2 = a.buf2 + sp.state_off;
-    if (sp.rk >= 2) {  // EULER, EULER_EQ: fluxes of the state itself
+    if (RK >= 2) {  // EULER, EULER_EQ: fluxes of the state itself
         if (type == 0)
             for (int p = 0; p < NPL; ++p) b2[(long long)p * sp.plane + o] = st[(long long)p * sp.plane + o];
         if (a.want_residual && type == 0) a.told[node] = node_macro(st, sp, o).T;
@@ -110,7 +112,7 @@ __global__ void __launch_bounds__(256) k_stage0(KArgs<S> a)
     }
     const C dt = (C)sp.dt, ux = (C)m.ux, uy = (C)m.uy;
     const C tf = (C)m.tf, th = (C)m.th, thf = (C)m.thf;
-    if (sp.rk == 1) {
+    if (RK == 1) {
         // RK3 stages 1 and 2 (cpuLBM.cpp:1819-1924); stage 2 reuses stage 1's
         // equilibrium, moments and relaxation times.
         const C cf = dt / (C(2) * tf), ch = dt / (C(2) * th), chf = dt / (C(2) * thf);
@@ -157,7 +159,7 @@ __global__ void k_wall(KArgs<S> a, const S *__restrict__ stage, const WallNode *
     if (k >= nwalls) return;
     const WallNode w = walls[k];
     const SampleParams sp = a.samples[w.sample];
-    const StageView<S> v{stage + sp.state_off, a.nflags + sp.node_off, sp.plane, sp.pitch};
+    const StageView<S> v{stage + sp.state_off, a.nflags + sp.node_off, (int)sp.plane, sp.pitch};
     const double dxm = a.dxv[sp.xoff + w.x], dym = a.dyv[sp.yoff + w.y];
     double fin = 0, fout = 0;
     for (int j = 0; j < 4; ++j) {
@@ -180,104 +182,314 @@ __global__ void k_wall(KArgs<S> a, const S *__restrict__ stage, const WallNode *
 }
 
 // ------------------------------------------------------------------ P1/P2
-// flux of plane p at a node, solid nodes answering alpha |e| f_stage
-// (wallFluxes' outgoing flux, cpuLBM.cpp:1576-1586)
+// Fast-path reconstruction along a line through c0 with element step `st`
+// (upwind ordering already folded into the sign of st).
 template <class S, class C>
-__device__ __forceinline__ C node_flux(const KArgs<S> &a, const SampleParams &sp, const StageView<S> &v, int x, int y,
-                                       int p, int axis)
+__device__ __forceinline__ C line_flux(const SampleParams &sp, const S *__restrict__ c0, int st, C ae)
 {
-    const long long o = (long long)y * sp.pitch + x;
-    const uint8_t fl = v.nf[o];
-    if ((fl & NF_TYPE) == 2) {
-        const int i = p < NQ ? p : p - NQ;
-        const C al = a.template alpha_as<C>()[sp.node_off + o];
-        return al * (C)(sp.c * abs(axis == 0 ? c_EX[i] : c_EY[i])) * (C)ldv(v, p, x, y);
-    }
-    return flux_axis<S, C>(sp, v, x, y, p, axis, fl);
+    if (sp.fm)
+        return weno5<C>(ae, (C)__ldg(c0 - 2 * st), (C)__ldg(c0 - st), (C)__ldg(c0), (C)__ldg(c0 + st),
+                        (C)__ldg(c0 + 2 * st));
+    return nnd3<C>(ae, (C)__ldg(c0 - st), (C)__ldg(c0), (C)__ldg(c0 + st));
 }
 
-template <class S, class C, int PH>
-__global__ void __launch_bounds__(256) k_flux(KArgs<S> a)
+// Stage tiles in shared memory: per direction the f and h planes over the
+// box [x0-4, x0+TX+4) x [y0-3, y0+TY+3) (x start kept on a 16-byte
+// boundary), loaded by TMA three directions ahead of use.
+constexpr int HALO_X = 4, HALO_Y = 3, NSTAGE = 3;
+constexpr uint32_t TMA_WAIT_POLLS = 1u << 16;
+
+// Shared-memory layout of k_flux (bytes from a 128-byte aligned base).
+struct FluxSmemLayout {
+    size_t c_elems;      // C arrays: sf[8NT], ring x[4TY], ring y[4TX], sD[26NT]
+    size_t stage_off;    // staged boxes
+    size_t plane_bytes;  // one staged plane, padded to 128 bytes
+    size_t bar_off;      // NSTAGE mbarriers
+    size_t total;        // including 128 bytes of base-alignment slack
+};
+
+__host__ __device__ inline FluxSmemLayout flux_layout(size_t es_c, size_t es_s, int tx, int ty)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FluxSmemLayout L;
+    const size_t NT = (size_t)tx * ty;
+    L.c_elems = 8 * NT + 4 * (size_t)tx + 4 * (size_t)ty + (size_t)NPL * NT;
+    L.stage_off = (L.c_elems * es_c + 127) / 128 * 128;
+    L.plane_bytes = ((size_t)(tx + 2 * HALO_X) * (ty + 2 * HALO_Y) * es_s + 127) / 128 * 128;
+    L.bar_off = L.stage_off + (size_t)NSTAGE * 2 * L.plane_bytes;
+    L.total = L.bar_off + NSTAGE * sizeof(uint64_t) + 128;
+    return L;
+}
+
+template <class S, class C>
+struct TileCtx {
+    const SampleParams *sp;
+    StageView<S> v;
+    const C *alpha;  // alpha of this sample (node-indexed)
+    C *sf;           // [2 buffers][4: fx_f, fx_h, fy_f, fy_h][NT]
+    C *ringx;        // [2 buffers][2: f, h][TY]
+    C *ringy;        // [2 buffers][2: f, h][TX]
+    C *sD;           // [26][NT]
+    const S *stg;    // [NSTAGE][2: f, h][BH][BW], planes `pstride` elements apart
+    int pstride;
+    uint64_t *bars;  // [NSTAGE]
+    const CUtensorMap *map;
+    int *timed_out;  // shared flag
+    int *status;     // this sample's status word
+    int NT, TX, TY, BW, BH, tid, tx, ty, x, y, x0, y0, x_end, y_end, o;
+    uint8_t flag;
+    bool active;
+    C tdx, tdy;
+};
+
+template <class S, class C>
+__device__ __forceinline__ void issue_dir_load(TileCtx<S, C> &k, int dir, int slot)
+{
+    const uint32_t box = (uint32_t)(k.BW * k.BH * sizeof(S));
+    S *dst = const_cast<S *>(k.stg) + (size_t)slot * 2 * k.pstride;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&k.bars[slot], 2 * box);
+    tma_load_3d(dst, k.map, k.x0 - HALO_X, k.y0 - HALO_Y, dir, &k.bars[slot]);
+    tma_load_3d(dst + k.pstride, k.map, k.x0 - HALO_X, k.y0 - HALO_Y, NQ + dir, &k.bars[slot]);
+}
+
+// reconstruction from the staged box (fast path; no solid, no domain edge
+// within the stencil): element step `st` in the box, upwind sign folded in
+template <class S, class C>
+__device__ __forceinline__ C box_flux(const SampleParams &sp, const S *c0, int st, C ae)
+{
+    if (sp.fm) return weno5<C>(ae, (C)c0[-2 * st], (C)c0[-st], (C)c0[0], (C)c0[st], (C)c0[2 * st]);
+    return nnd3<C>(ae, (C)c0[-st], (C)c0[0], (C)c0[st]);
+}
+
+// Flux of plane slot fh (0 f, 1 h) of direction i at node (xn, yn), along
+// `axis`: solid nodes answer alpha |e| f; nodes whose stencil stays in the
+// staged box and meets no solid/edge read the box; the rest run the wrapped
+// or the exact boundary-aware stencil on global memory.  `mirrored`
+// selects the reflected plane (cFLUX at a mirror boundary).
+template <class S, class C>
+__device__ __forceinline__ C any_node_flux(TileCtx<S, C> &k, const S *box, int i, int xn, int yn, int fh, int axis,
+                                          bool mirrored, bool in_box)
+{
+    const SampleParams &sp = *k.sp;
+    const int ev = axis == 0 ? c_EX[i] : c_EY[i];
+    const int pp = fh * NQ + (mirrored ? (axis == 0 ? c_MIR_EW[i] : c_MIR_NS[i]) : i);
+    const int oo = yn * k.v.pitch + xn;
+    const uint8_t fl = k.v.nf[oo];
+    const C ae = (C)(sp.c * (double)abs(ev));
+    if ((fl & NF_TYPE) == 2) return k.alpha[oo] * ae * (C)__ldg(k.v.st + (pp * k.v.plane + oo));
+    const uint8_t edge = axis == 0 ? (NF_SOLX | NF_EDGX | NF_WRPX) : (NF_SOLY | NF_EDGY | NF_WRPY);
+    if (in_box && !mirrored && !(fl & edge)) {
+        const int lx = xn - (k.x0 - HALO_X), ly = yn - (k.y0 - HALO_Y);
+        const S *c0 = box + (size_t)fh * k.pstride + ly * k.BW + lx;
+        const int e = ev > 0 ? 1 : -1;
+        return box_flux<S, C>(sp, c0, axis == 0 ? e : e * k.BW, ae);
+    }
+    return flux_axis<S, C>(sp, k.v, xn, yn, pp, axis, fl);
+}
+
+// Direction i (1..12): outgoing face fluxes of the f and h planes at this
+// node (posFluxes/computeFlux, cpuLBM.cpp:1405-1500; a solid node answers
+// wallFluxes' alpha |e| f, cpuLBM.cpp:1576-1586), the upwind fluxes across
+// the tile edges, then the divergence D = (dt/dx, dt/dy).(F_out - F_in) of
+// cFLUX (cpuLBM.cpp:1436-1470).  One copy of the code serves all twelve
+// directions (a compact loop keeps the instruction cache warm).
+template <class S, class C>
+__device__ __forceinline__ void dir_step(TileCtx<S, C> &k, const int i)
+{
+    const int EX = c_EX[i], EY = c_EY[i];
+    const int SX = isgn(EX), SY = isgn(EY);
+    const int buf = i & 1;
+    const int slot = (i - 1) % NSTAGE;
+    const uint32_t parity = ((i - 1) / NSTAGE) & 1;
+    const int NT = k.NT;
+    C *sf = k.sf + buf * 4 * NT;
+    C *ringx = k.ringx + buf * 2 * k.TY;
+    C *ringy = k.ringy + buf * 2 * k.TX;
+    const S *box = k.stg + (size_t)slot * 2 * k.pstride;
+    // every issued copy is waited for (boundedly), also after a timeout, so
+    // no copy is still in flight when the block exits
+    if (!mbar_wait_bounded(&k.bars[slot], parity, TMA_WAIT_POLLS)) {
+        *k.timed_out = 1;
+        atomicOr(k.status, STATUS_TIMEOUT);
+    }
+    const SampleParams &sp = *k.sp;
+    if (k.active) {
+        const int type = k.flag & NF_TYPE;
+        const C c = (C)sp.c;
+        const C aex = C(abs(EX)) * c, aey = C(abs(EY)) * c;
+        const int lx = k.tx + HALO_X, ly = k.ty + HALO_Y;
+        const S *cf = box + ly * k.BW + lx;
+        const S *ch = cf + k.pstride;
+        if (type == 2) {
+            const C al = k.alpha[k.o];
+            const C fv = (C)cf[0], hv = (C)ch[0];
+            if (SX) { sf[k.tid] = al * aex * fv; sf[NT + k.tid] = al * aex * hv; }
+            if (SY) { sf[2 * NT + k.tid] = al * aey * fv; sf[3 * NT + k.tid] = al * aey * hv; }
+        } else {
+            if (SX) {
+                C a, b;
+                if (k.flag & (NF_SOLX | NF_EDGX | NF_WRPX)) {
+                    a = flux_axis<S, C>(sp, k.v, k.x, k.y, i, 0, k.flag);
+                    b = flux_axis<S, C>(sp, k.v, k.x, k.y, NQ + i, 0, k.flag);
+                } else {
+                    a = box_flux<S, C>(sp, cf, SX, aex);
+                    b = box_flux<S, C>(sp, ch, SX, aex);
+                }
+                sf[k.tid] = a;
+                sf[NT + k.tid] = b;
+            }
+            if (SY) {
+                C a, b;
+                if (k.flag & (NF_SOLY | NF_EDGY | NF_WRPY)) {
+                    a = flux_axis<S, C>(sp, k.v, k.x, k.y, i, 1, k.flag);
+                    b = flux_axis<S, C>(sp, k.v, k.x, k.y, NQ + i, 1, k.flag);
+                } else {
+                    a = box_flux<S, C>(sp, cf, SY * k.BW, aey);
+                    b = box_flux<S, C>(sp, ch, SY * k.BW, aey);
+                }
+                sf[2 * NT + k.tid] = a;
+                sf[3 * NT + k.tid] = b;
+            }
+        }
+    }
+    // upwind neighbours outside the tile: index(x, -e) with reflection
+    {
+        const int nx_items = SX ? 2 * k.TY : 0, ny_items = SY ? 2 * k.TX : 0;
+        const int r = k.tid;
+        if (r < nx_items) {
+            const int fh = r / k.TY, row = r % k.TY, yy = k.y0 + row;
+            C val = C(0);
+            if (yy < k.y_end) {
+                int m;
+                const int xn = SX > 0 ? k.x0 : k.x_end - 1;
+                const int xr = bc_index(sp, xn, -SX, 0, m);
+                const bool in_box = !m && xr == xn - SX;
+                val = any_node_flux<S, C>(k, box, i, xr, yy, fh, 0, m != 0, in_box);
+            }
+            ringx[fh * k.TY + row] = val;
+        } else if (r < nx_items + ny_items) {
+            const int q = r - nx_items, fh = q / k.TX, col = q % k.TX, xx = k.x0 + col;
+            C val = C(0);
+            if (xx < k.x_end) {
+                int m;
+                const int yn = SY > 0 ? k.y0 : k.y_end - 1;
+                const int yr = bc_index(sp, yn, -SY, 1, m);
+                const bool in_box = !m && yr == yn - SY;
+                val = any_node_flux<S, C>(k, box, i, xx, yr, fh, 1, m != 0, in_box);
+            }
+            ringy[fh * k.TX + col] = val;
+        }
+    }
+    __syncthreads();
+    // every thread is done with this slot: refill it three directions ahead
+    if (i + NSTAGE <= 12 && k.tid == 0) issue_dir_load(k, i + NSTAGE, slot);
+    if (k.active && (k.flag & NF_TYPE) == 0) {
+        C of = C(0), oh = C(0), inf_ = C(0), inh = C(0);
+        bool have = false;
+        if (SX) {
+            const int xu = k.x - SX;
+            const bool inside = xu >= k.x0 && xu < k.x_end;
+            const C fi = inside ? sf[k.tid - SX] : ringx[k.ty];
+            const C hi = inside ? sf[NT + k.tid - SX] : ringx[k.TY + k.ty];
+            of = k.tdx * sf[k.tid];
+            oh = k.tdx * sf[NT + k.tid];
+            inf_ = k.tdx * fi;
+            inh = k.tdx * hi;
+            have = true;
+        }
+        if (SY) {
+            const int yu = k.y - SY;
+            const bool inside = yu >= k.y0 && yu < k.y_end;
+            const C fi = inside ? sf[2 * NT + k.tid - SY * k.TX] : ringy[k.tx];
+            const C hi = inside ? sf[3 * NT + k.tid - SY * k.TX] : ringy[k.TX + k.tx];
+            if (have) {
+                of = of + k.tdy * sf[2 * NT + k.tid];
+                oh = oh + k.tdy * sf[3 * NT + k.tid];
+                inf_ = inf_ + k.tdy * fi;
+                inh = inh + k.tdy * hi;
+            } else {
+                of = k.tdy * sf[2 * NT + k.tid];
+                oh = k.tdy * sf[3 * NT + k.tid];
+                inf_ = k.tdy * fi;
+                inh = k.tdy * hi;
+            }
+        }
+        k.sD[i * NT + k.tid] = of - inf_;
+        k.sD[(NQ + i) * NT + k.tid] = oh - inh;
+    }
+    // sf and the rings are double-buffered by direction parity: buffer
+    // (i & 1) is written again at direction i + 2, after direction i + 1's
+    // barrier, which every reader of this direction has passed.
+}
+
+size_t flux_smem_bytes_t(size_t es, int tx, int ty) { return flux_layout(es, es, tx, ty).total; }
+
+// MODE: 1 = RK3 stage 3 (fluxes of buffer 2), 2 = RK3 final (buffer 3),
+// 3 = RK1 update, 4 = EULER update, 5 = EULER_EQ update (buffer 2)
+template <class S, class C, int MODE>
+__global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
+{
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
     const int TX = a.tx, TY = a.ty, NT = TX * TY;
-    C *sfx = reinterpret_cast<C *>(smem_raw);  // [2][NT]
-    C *sfy = sfx + 2 * NT;                      // [2][NT]
-    C *ringx = sfy + 2 * NT;                    // [26][TY]
-    C *ringy = ringx + NPL * TY;                // [26][TX]
-    C *sD = ringy + NPL * TX;                   // [26][NT]
+    const int BW = TX + 2 * HALO_X, BH = TY + 2 * HALO_Y;
+    const FluxSmemLayout Ls = flux_layout(sizeof(C), sizeof(S), TX, TY);
+    unsigned char *smem_raw = smem_dyn + ((128 - (smem_u32(smem_dyn) & 127)) & 127);
+    C *sf = reinterpret_cast<C *>(smem_raw);  // [2][4][NT]
+    C *ringx = sf + 8 * NT;                    // [2][2][TY]
+    C *ringy = ringx + 4 * TY;                 // [2][2][TX]
+    C *sD = ringy + 4 * TX;                    // [26][NT]
+    S *stg = reinterpret_cast<S *>(smem_raw + Ls.stage_off);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + Ls.bar_off);
     __shared__ double red[32];
+    __shared__ SampleParams s_sp;  // kept out of registers: read as needed
+    __shared__ int s_timeout;
 
     const Tile t = a.tiles[blockIdx.x];
-    const SampleParams sp = a.samples[t.sample];
     const int tid = threadIdx.x;
+    constexpr int PH = MODE == 2 ? 2 : 1;
+    const CUtensorMap *map = a.tmaps + 2 * t.sample + (PH == 1 ? 0 : 1);
+
+    TileCtx<S, C> k;
+    k.NT = NT; k.TX = TX; k.TY = TY; k.BW = BW; k.BH = BH; k.tid = tid;
+    k.x0 = t.x0; k.y0 = t.y0;
+    k.stg = stg; k.pstride = (int)(Ls.plane_bytes / sizeof(S)); k.bars = bars; k.map = map; k.timed_out = &s_timeout;
+    if (tid == 0) {
+        s_sp = a.samples[t.sample];
+        s_timeout = 0;
+        for (int b = 0; b < NSTAGE; ++b) mbar_init(&bars[b], 1);
+        fence_mbar_init();
+        for (int d = 1; d <= NSTAGE; ++d) issue_dir_load(k, d, d - 1);
+    }
+    __syncthreads();
+    const SampleParams &sp = s_sp;
     const int tx = tid % TX, ty = tid / TX;
     const int x = t.x0 + tx, y = t.y0 + ty;
     const int x_end = min(t.x0 + TX, sp.nx), y_end = min(t.y0 + TY, sp.ny);
     const bool active = x < sp.nx && y < sp.ny;
     const S *stage = PH == 1 ? a.buf2 : a.buf3;
-    const StageView<S> v{stage + sp.state_off, a.nflags + sp.node_off, sp.plane, sp.pitch};
-    const long long o = (long long)y * sp.pitch + x;
-    const uint8_t myflag = active ? v.nf[o] : 0;
-    const int type = myflag & NF_TYPE;
+    const StageView<S> v{stage + sp.state_off, a.nflags + sp.node_off, (int)sp.plane, sp.pitch};
+    const int o = y * sp.pitch + x;
+    const C *alpha = a.template alpha_as<C>() + sp.node_off;
 
-    // upwind fluxes across the tile edges, for all planes (cFLUX's
-    // index(x, -e) neighbour with its reflected direction, cpuLBM.cpp:1436-1470)
-    for (int r = tid; r < NPL * (TX + TY); r += NT) {
-        const int p = r / (TX + TY), k = r % (TX + TY);
-        const int i = p < NQ ? p : p - NQ, pb = p - i;
-        C val = C(0);
-        if (k < TY) {
-            const int yy = t.y0 + k, e = isgn(c_EX[i]);
-            if (yy < y_end && e != 0) {
-                int m;
-                const int xn = e > 0 ? t.x0 : x_end - 1;
-                const int xr = bc_index(sp, xn, -e, 0, m);
-                val = node_flux<S, C>(a, sp, v, xr, yy, m ? pb + c_MIR_EW[i] : p, 0);
-            }
-            ringx[p * TY + k] = val;
-        } else {
-            const int xx = t.x0 + (k - TY), e = isgn(c_EY[i]);
-            if (xx < x_end && e != 0) {
-                int m;
-                const int yn = e > 0 ? t.y0 : y_end - 1;
-                const int yr = bc_index(sp, yn, -e, 1, m);
-                val = node_flux<S, C>(a, sp, v, xx, yr, m ? pb + c_MIR_NS[i] : p, 1);
-            }
-            ringy[p * TX + (k - TY)] = val;
-        }
-    }
-
-    const C tdx = active ? (C)a.tdx[sp.xoff + x] : C(0);
-    const C tdy = active ? (C)a.tdy[sp.yoff + y] : C(0);
-    for (int p = 0; p < NPL; ++p) {
-        const int buf = p & 1;
-        const int i = p < NQ ? p : p - NQ;
-        if (active) {
-            C Fx, Fy;
-            if (type == 2) {
-                const C al = a.template alpha_as<C>()[sp.node_off + o];
-                const C sv = (C)ldv(v, p, x, y);
-                Fx = al * (C)(sp.c * abs(c_EX[i])) * sv;
-                Fy = al * (C)(sp.c * abs(c_EY[i])) * sv;
-            } else {
-                Fx = flux_axis<S, C>(sp, v, x, y, p, 0, myflag);
-                Fy = flux_axis<S, C>(sp, v, x, y, p, 1, myflag);
-            }
-            sfx[buf * NT + tid] = Fx;
-            sfy[buf * NT + tid] = Fy;
-        }
-        __syncthreads();
-        if (active && type == 0) {
-            const int ex = isgn(c_EX[i]), ey = isgn(c_EY[i]);
-            const int xu = x - ex, yu = y - ey;
-            const C Fx_in = (xu >= t.x0 && xu < x_end) ? sfx[buf * NT + ty * TX + (xu - t.x0)] : ringx[p * TY + ty];
-            const C Fy_in = (yu >= t.y0 && yu < y_end) ? sfy[buf * NT + (yu - t.y0) * TX + tx] : ringy[p * TX + tx];
-            const C out = tdx * sfx[buf * NT + tid] + tdy * sfy[buf * NT + tid];
-            const C in = tdx * Fx_in + tdy * Fy_in;
-            sD[p * NT + tid] = out - in;
-        }
-    }
+    k.sp = &sp;
+    k.v = v;
+    k.alpha = alpha;
+    k.sf = sf;
+    k.ringx = ringx;
+    k.ringy = ringy;
+    k.sD = sD;
+    k.status = &a.status[t.sample];
+    k.tx = tx; k.ty = ty; k.x = x; k.y = y;
+    k.x_end = x_end; k.y_end = y_end; k.o = o;
+    k.active = active;
+    k.flag = active ? v.nf[o] : 0;
+    k.tdx = active ? (C)a.tdx[sp.xoff + x] : C(0);
+    k.tdy = active ? (C)a.tdy[sp.yoff + y] : C(0);
+    const int type = k.flag & NF_TYPE;
+    sD[tid] = C(0);          // direction 0 streams nothing
+    sD[NQ * NT + tid] = C(0);
+#pragma unroll 1
+    for (int i = 1; i <= 12; ++i) dir_step<S, C>(k, i);
 
     double res_part = 0;
     if (active && type == 0) {
@@ -286,29 +498,43 @@ __global__ void __launch_bounds__(256) k_flux(KArgs<S> a)
         S *b3 = a.buf3 + sp.state_off;
         const C dt = (C)sp.dt;
         bool final_phase = true;
-        if (PH == 1 && sp.rk == 1) {
+        if (MODE == 1) {
             // RK3 stage 3 (cpuLBM.cpp:1928-1993) and the part of the update
             // (cpuLBM.cpp:1999-2042) that does not need the stage-3 fluxes
             final_phase = false;
-            const Macro m1 = node_macro(st, sp, o);
-            double r = 0, rux = 0, ruy = 0, sh = 0;
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) {
-                const double fv = (double)st[(long long)i * sp.plane + o];
-                const double Df = (double)sD[i * NT + tid];
-                r += fv - Df;
-                rux += fv * (sp.c * c_EX[i]) - Df * (sp.c * c_EX[i]);
-                ruy += fv * (sp.c * c_EY[i]) - Df * (sp.c * c_EY[i]);
-                sh += (double)st[(long long)(NQ + i) * sp.plane + o] - (double)sD[(NQ + i) * NT + tid];
+            // stage-1 moments (= stage 2's) and the moments of f - div F(f2)
+            // (macroProp3, cpuLBM.cpp:973-1032), both summed in FP64
+            EqState<C> q1, q3;
+            C tf2, th2, thf2, tf3, th3, thf3, ux1, uy1, ux3, uy3;
+            double rho3;
+            {
+                const Macro m1 = node_macro(st, sp, o);
+                q1 = eq_state<C>(m1.rho, m1.ux, m1.uy, m1.T, sp);
+                tf2 = (C)m1.tf; th2 = (C)m1.th; thf2 = (C)m1.thf; ux1 = (C)m1.ux; uy1 = (C)m1.uy;
             }
-            const Macro m3 = macro_from_sums(r, rux, ruy, sh, sp);
-            const EqState<C> q1 = eq_state<C>(m1.rho, m1.ux, m1.uy, m1.T, sp);
-            const EqState<C> q3 = eq_state<C>(m3.rho, m3.ux, m3.uy, m3.T, sp);
-            const C tf2 = (C)m1.tf, th2 = (C)m1.th, thf2 = (C)m1.thf;
-            const C tf3 = (C)m3.tf, th3 = (C)m3.th, thf3 = (C)m3.thf;
-            const C a2 = dt / (C(2) * tf2), a3 = dt / (C(2) * tf3), b2c = dt / (C(2) * th2), b3c = dt / (C(2) * th3);
-            const C ux1 = (C)m1.ux, uy1 = (C)m1.uy, ux3 = (C)m3.ux, uy3 = (C)m3.uy;
+            {
+                double r = 0, rux = 0, ruy = 0, sh = 0;
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) {
+                    const double fv = (double)st[(long long)i * sp.plane + o];
+                    const double Df = (double)sD[i * NT + tid];
+                    r += fv - Df;
+                    rux += fv * (sp.c * c_EX[i]) - Df * (sp.c * c_EX[i]);
+                    ruy += fv * (sp.c * c_EY[i]) - Df * (sp.c * c_EY[i]);
+                    sh += (double)st[(long long)(NQ + i) * sp.plane + o] - (double)sD[(NQ + i) * NT + tid];
+                }
+                const Macro m3 = macro_from_sums(r, rux, ruy, sh, sp);
+                q3 = eq_state<C>(m3.rho, m3.ux, m3.uy, m3.T, sp);
+                tf3 = (C)m3.tf; th3 = (C)m3.th; thf3 = (C)m3.thf; ux3 = (C)m3.ux; uy3 = (C)m3.uy;
+                rho3 = m3.rho;
+            }
+            const C hdt = dt * C(0.5);
+            const C a2 = hdt / tf2, a3 = hdt / tf3, b2c = hdt / th2, b3c = hdt / th3;
+            const C ia3 = C(1) / (C(1) + a3), ib3 = C(1) / (C(1) + b3c);
+            const C g2 = C(1) / thf2, g3 = C(1) / thf3, itf2 = C(1) / tf2, itf3 = C(1) / tf3;
+            const C ith2 = C(1) / th2, ith3 = C(1) / th3;
             double sf3 = 0;
+#pragma unroll 1
             for (int fam = 0; fam < 4; ++fam) {
                 C e1f[4], e1h[4], e3f[4], e3h[4];
                 int i0, n;
@@ -316,7 +542,9 @@ __global__ void __launch_bounds__(256) k_flux(KArgs<S> a)
                 else if (fam == 1) { eq_fam1(q1, e1f, e1h); eq_fam1(q3, e3f, e3h); i0 = 1; n = 4; }
                 else if (fam == 2) { eq_fam5(q1, e1f, e1h); eq_fam5(q3, e3f, e3h); i0 = 5; n = 4; }
                 else { eq_fam9(q1, e1f, e1h); eq_fam9(q3, e3f, e3h); i0 = 9; n = 4; }
-                for (int k = 0; k < n; ++k) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (k >= n) break;
                     const int i = i0 + k;
                     sf3 += (double)e3f[k];
                     const long long of = (long long)i * sp.plane + o, oh = (long long)(NQ + i) * sp.plane + o;
@@ -324,21 +552,22 @@ __global__ void __launch_bounds__(256) k_flux(KArgs<S> a)
                     const C Df = sD[i * NT + tid], Dh = sD[(NQ + i) * NT + tid];
                     const C exi = (C)(sp.c * c_EX[i]), eyi = (C)(sp.c * c_EY[i]);
                     const C eu2 = exi * ux1 + eyi * uy1, eu3 = exi * ux3 + eyi * uy3;
-                    const C f3 = (f - Df + a2 * (e1f[k] - f2) + a3 * e3f[k]) / (C(1) + a3);
-                    const C h3 = (h - Dh - (dt / C(2)) * ((eu2 / thf2) * (e1f[k] - f2) + (eu3 / thf3) * (e3f[k] - f3))
-                                  + b2c * (e1h[k] - h2) + b3c * e3h[k]) / (C(1) + b3c);
-                    const C accf = f - C(0.5) * Df + (dt / C(2)) * ((e1f[k] - f2) / tf2 + (e3f[k] - f3) / tf3);
-                    const C acch = h - C(0.5) * Dh + (dt / C(2)) * ((e1h[k] - h2) / th2 + (e3h[k] - h3) / th3)
-                                   - (dt / C(2)) * ((eu2 / thf2) * (e1f[k] - f2) + (eu3 / thf3) * (e3f[k] - f3));
+                    // stage 3 (cpuLBM.cpp:1970, 1986)
+                    const C f3 = (f - Df + a2 * (e1f[k] - f2) + a3 * e3f[k]) * ia3;
+                    const C cpl = eu2 * g2 * (e1f[k] - f2) + eu3 * g3 * (e3f[k] - f3);
+                    const C h3 = (h - Dh - hdt * cpl + b2c * (e1h[k] - h2) + b3c * e3h[k]) * ib3;
+                    // update without the stage-3 fluxes (cpuLBM.cpp:2022, 2039)
+                    const C accf = f - C(0.5) * Df + hdt * ((e1f[k] - f2) * itf2 + (e3f[k] - f3) * itf3);
+                    const C acch = h - C(0.5) * Dh + hdt * ((e1h[k] - h2) * ith2 + (e3h[k] - h3) * ith3) - hdt * cpl;
                     b3[of] = (S)f3;
                     b3[oh] = (S)h3;
                     st[of] = (S)accf;
                     st[oh] = (S)acch;
                 }
             }
-            if (fabs(sf3 - m3.rho) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(m3.rho))))
+            if (fabs(sf3 - rho3) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(rho3))))
                 atomicOr(&a.status[t.sample], STATUS_EQ);
-        } else if (PH == 2) {
+        } else if (MODE == 2) {
             // final RK3 combination (cpuLBM.cpp:1999-2042): f = acc - D3/2
             for (int p = 0; p < NPL; ++p) {
                 const long long op = (long long)p * sp.plane + o;
@@ -348,37 +577,43 @@ __global__ void __launch_bounds__(256) k_flux(KArgs<S> a)
             // RK1 update (cpuLBM.cpp:1674-1710), EULER (:2130-2168), EULER_EQ (:2220-2258)
             const Macro m = node_macro(st, sp, o);
             const EqState<C> q = eq_state<C>(m.rho, m.ux, m.uy, m.T, sp);
-            C fe[NQ], he[NQ];
-            eq_all(q, fe, he);
-            if (sp.rk >= 2) {
-                double sf = 0;
-#pragma unroll
-                for (int i = 0; i < NQ; ++i) sf += (double)fe[i];
-                if (fabs(sf - m.rho) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(m.rho))))
-                    atomicOr(&a.status[t.sample], STATUS_EQ);
-            }
             const C tf = (C)m.tf, th = (C)m.th, thf = (C)m.thf, ux = (C)m.ux, uy = (C)m.uy;
+            double sf = 0;
+#pragma unroll 1
+            for (int fam = 0; fam < 4; ++fam) {
+                C fe[4], he[4];
+                int i0, n;
+                if (fam == 0) { eq_fam0(q, fe[0], he[0]); i0 = 0; n = 1; }
+                else if (fam == 1) { eq_fam1(q, fe, he); i0 = 1; n = 4; }
+                else if (fam == 2) { eq_fam5(q, fe, he); i0 = 5; n = 4; }
+                else { eq_fam9(q, fe, he); i0 = 9; n = 4; }
 #pragma unroll
-            for (int i = 0; i < NQ; ++i) {
-                const long long of = (long long)i * sp.plane + o, oh = (long long)(NQ + i) * sp.plane + o;
-                const C f = (C)st[of], h = (C)st[oh];
-                const C Df = sD[i * NT + tid], Dh = sD[(NQ + i) * NT + tid];
-                const C eu = (C)(sp.c * c_EX[i]) * ux + (C)(sp.c * c_EY[i]) * uy;
-                C fn, hn;
-                if (sp.rk == 0) {
-                    const C f1 = (C)b2[of], h1 = (C)b2[oh];
-                    fn = f - Df + (dt / tf) * (fe[i] - f1);
-                    hn = h - Dh + (dt / th) * (he[i] - h1) - ((dt * eu) / thf) * (fe[i] - f1);
-                } else if (sp.rk == 2) {
-                    fn = f - Df + (dt / tf) * (fe[i] - f);
-                    hn = h - Dh + (dt / th) * (he[i] - h) - ((dt * eu) / thf) * (fe[i] - f);
-                } else {
-                    fn = fe[i] - Df;
-                    hn = he[i] - Dh;
+                for (int k = 0; k < 4; ++k) {
+                    if (k >= n) break;
+                    const int i = i0 + k;
+                    sf += (double)fe[k];
+                    const long long of = (long long)i * sp.plane + o, oh = (long long)(NQ + i) * sp.plane + o;
+                    const C f = (C)st[of], h = (C)st[oh];
+                    const C Df = sD[i * NT + tid], Dh = sD[(NQ + i) * NT + tid];
+                    const C eu = (C)(sp.c * c_EX[i]) * ux + (C)(sp.c * c_EY[i]) * uy;
+                    C fn, hn;
+                    if (MODE == 3) {
+                        const C f1 = (C)b2[of], h1 = (C)b2[oh];
+                        fn = f - Df + (dt / tf) * (fe[k] - f1);
+                        hn = h - Dh + (dt / th) * (he[k] - h1) - ((dt * eu) / thf) * (fe[k] - f1);
+                    } else if (MODE == 4) {
+                        fn = f - Df + (dt / tf) * (fe[k] - f);
+                        hn = h - Dh + (dt / th) * (he[k] - h) - ((dt * eu) / thf) * (fe[k] - f);
+                    } else {
+                        fn = fe[k] - Df;
+                        hn = he[k] - Dh;
+                    }
+                    st[of] = (S)fn;
+                    st[oh] = (S)hn;
                 }
-                st[of] = (S)fn;
-                st[oh] = (S)hn;
             }
+            if (MODE >= 4 && fabs(sf - m.rho) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(m.rho))))
+                atomicOr(&a.status[t.sample], STATUS_EQ);
         }
         if (final_phase) {
             // macroPropShort of the new state: the residual's T and a
@@ -392,7 +627,7 @@ __global__ void __launch_bounds__(256) k_flux(KArgs<S> a)
             }
         }
     }
-    if (a.want_residual && ((PH == 2) || (PH == 1 && sp.rk != 1))) {
+    if (a.want_residual && MODE != 1) {
         // per-tile partial sum, fixed order (deterministic)
         for (int off = 16; off > 0; off >>= 1) res_part += __shfl_down_sync(0xffffffffu, res_part, off);
         if ((tid & 31) == 0) red[tid >> 5] = res_part;
@@ -465,9 +700,52 @@ __global__ void k_dist_io(const SampleParams *samples, int s, S *state, S *buf2,
     }
 }
 
+// f, h = equilibria of per-node fields given in [x*Ny + y] order (FP64)
+template <class S>
+__global__ void k_set_macro(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, const double *fields,
+                            const uint8_t *nflags)
+{
+    const SampleParams sp = samples[s];
+    const long long n = (long long)sp.nx * sp.ny;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(k % sp.ny), x = (int)(k / sp.ny);
+        const EqState<double> q = eq_state<double>(fields[k], fields[n + k], fields[2 * n + k], fields[3 * n + k], sp);
+        double f[NQ], h[NQ];
+        eq_all(q, f, h);
+        const long long o = (long long)y * sp.pitch + x;
+        const bool fixed = (nflags[sp.node_off + o] & NF_TYPE) != 0;
+        for (int i = 0; i < NQ; ++i) {
+            const long long of = sp.state_off + (long long)i * sp.plane + o;
+            const long long oh = sp.state_off + (long long)(NQ + i) * sp.plane + o;
+            state[of] = (S)f[i];
+            state[oh] = (S)h[i];
+            if (fixed) {
+                buf2[of] = (S)f[i]; buf3[of] = (S)f[i];
+                buf2[oh] = (S)h[i]; buf3[oh] = (S)h[i];
+            }
+        }
+    }
+}
+
+template <class S>
+cudaError_t launch_set_macro(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, const double *fields,
+                             const uint8_t *nflags, long long nodes, cudaStream_t st)
+{
+    const int blocks = (int)std::min<long long>((nodes + 255) / 256, 4096);
+    k_set_macro<S><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(samples, s, state, buf2, buf3, fields, nflags);
+    return cudaGetLastError();
+}
+template cudaError_t launch_set_macro<double>(const SampleParams *, int, double *, double *, double *, const double *,
+                                              const uint8_t *, long long, cudaStream_t);
+template cudaError_t launch_set_macro<float>(const SampleParams *, int, float *, float *, float *, const double *,
+                                             const uint8_t *, long long, cudaStream_t);
+
 // ----------------------------------------------------------------- launchers
+// phase: 0 pointwise stages, 1 stencil phase over buffer 2, 2 RK3 final
+// stencil phase over buffer 3, 3/4 wall fluxes of buffer 2/3.  rk selects
+// the method of the tiles passed (one method per launch).
 template <class S, class C>
-cudaError_t launch_phase(const KArgs<S> &a, int phase, const Tile *tiles, int ntiles, const WallNode *walls,
+cudaError_t launch_phase(const KArgs<S> &a, int phase, int rk, const Tile *tiles, int ntiles, const WallNode *walls,
                          int nwalls, cudaStream_t st)
 {
     KArgs<S> k = a;
@@ -475,14 +753,19 @@ cudaError_t launch_phase(const KArgs<S> &a, int phase, const Tile *tiles, int nt
     k.ntiles = ntiles;
     const int NT = a.tx * a.ty;
     if (phase == 0) {
-        if (ntiles) k_stage0<S, C><<<ntiles, NT, 0, st>>>(k);
+        if (!ntiles) return cudaSuccess;
+        if (rk == 1) k_stage0<S, C, 1><<<ntiles, NT, 0, st>>>(k);
+        else if (rk == 0) k_stage0<S, C, 0><<<ntiles, NT, 0, st>>>(k);
+        else k_stage0<S, C, 2><<<ntiles, NT, 0, st>>>(k);
     } else if (phase == 1 || phase == 2) {
-        const size_t sm = sizeof(C) * ((size_t)4 * NT + (size_t)NPL * (a.tx + a.ty) + (size_t)NPL * NT);
-        if (ntiles) {
-            if (phase == 1) k_flux<S, C, 1><<<ntiles, NT, sm, st>>>(k);
-            else k_flux<S, C, 2><<<ntiles, NT, sm, st>>>(k);
-        }
-    } else if (phase == 3 || phase == 4) {  // walls of buffer 2 / buffer 3
+        if (!ntiles) return cudaSuccess;
+        const size_t sm = flux_smem_bytes_t(sizeof(S), a.tx, a.ty);
+        if (phase == 2) k_flux<S, C, 2><<<ntiles, NT, sm, st>>>(k);
+        else if (rk == 1) k_flux<S, C, 1><<<ntiles, NT, sm, st>>>(k);
+        else if (rk == 0) k_flux<S, C, 3><<<ntiles, NT, sm, st>>>(k);
+        else if (rk == 2) k_flux<S, C, 4><<<ntiles, NT, sm, st>>>(k);
+        else k_flux<S, C, 5><<<ntiles, NT, sm, st>>>(k);
+    } else if (phase == 3 || phase == 4) {
         if (nwalls) k_wall<S, C><<<(nwalls + 127) / 128, 128, 0, st>>>(k, phase == 3 ? a.buf2 : a.buf3, walls, nwalls);
     }
     return cudaGetLastError();
@@ -492,16 +775,16 @@ template <class S, class C>
 cudaError_t prepare_kernels()
 {
     const int maxsm = 200 * 1024;
-    cudaError_t e = cudaFuncSetAttribute(k_flux<S, C, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_flux<S, C, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+    return e;
 }
 
-size_t flux_smem_bytes(int prec, int tx, int ty)
-{
-    const size_t NT = (size_t)tx * ty;
-    return (prec == 0 ? 8 : 4) * (4 * NT + (size_t)NPL * (tx + ty) + (size_t)NPL * NT);
-}
+size_t flux_smem_bytes(int prec, int tx, int ty) { return flux_smem_bytes_t(prec == 0 ? 8 : 4, tx, ty); }
 
 template <class S>
 cudaError_t launch_init(const KArgs<S> &a, const double *rho, const double *ux, const double *uy, const double *T,
@@ -536,9 +819,9 @@ cudaError_t launch_residual(const SampleParams *samples, int nsamples, const dou
     return cudaGetLastError();
 }
 
-template cudaError_t launch_phase<double, double>(const KArgs<double> &, int, const Tile *, int, const WallNode *, int,
-                                                  cudaStream_t);
-template cudaError_t launch_phase<float, float>(const KArgs<float> &, int, const Tile *, int, const WallNode *, int,
+template cudaError_t launch_phase<double, double>(const KArgs<double> &, int, int, const Tile *, int, const WallNode *,
+                                                  int, cudaStream_t);
+template cudaError_t launch_phase<float, float>(const KArgs<float> &, int, int, const Tile *, int, const WallNode *, int,
                                                 cudaStream_t);
 template cudaError_t prepare_kernels<double, double>();
 template cudaError_t prepare_kernels<float, float>();

@@ -1,6 +1,7 @@
 // Host-visible kernel interface of the D2Q13 LBM step (see lbm_kernels.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -13,6 +14,7 @@ struct Tile;
 
 constexpr int STATUS_EQ = 1;         // equilibrium mass check (cpuLBM.cpp:839-843)
 constexpr int STATUS_NONFINITE = 2;  // NaN / Inf / rho <= 0 in the state
+constexpr int STATUS_TIMEOUT = 4;    // a bounded device-side wait ran out
 
 struct WallNode {
     int sample, x, y, pad;
@@ -34,6 +36,7 @@ struct KArgs {
     double *partial;  // per-tile residual partial sums
     int *status;      // per-sample status bits
     const double *tdx, *tdy, *dxv, *dyv;
+    const CUtensorMap *tmaps;  // per sample: [buffer 2, buffer 3]
     int want_residual;
     double eq_tol;
 #ifdef __CUDACC__
@@ -44,7 +47,7 @@ struct KArgs {
 };
 
 template <class S, class C>
-cudaError_t launch_phase(const KArgs<S> &a, int phase, const Tile *tiles, int ntiles, const WallNode *walls,
+cudaError_t launch_phase(const KArgs<S> &a, int phase, int rk, const Tile *tiles, int ntiles, const WallNode *walls,
                          int nwalls, cudaStream_t st);
 template <class S, class C>
 cudaError_t prepare_kernels();
@@ -58,6 +61,9 @@ cudaError_t launch_macro_out(const SampleParams *samples, int s, const S *state,
 template <class S>
 cudaError_t launch_dist_io(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, double *aos, int to_aos,
                            const uint8_t *nflags, long long nodes, cudaStream_t st);
+template <class S>
+cudaError_t launch_set_macro(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, const double *fields,
+                             const uint8_t *nflags, long long nodes, cudaStream_t st);
 cudaError_t launch_residual(const SampleParams *samples, int nsamples, const double *partial, const int *tile_first,
                             const int *tile_count, double *residual, cudaStream_t st);
 

@@ -234,3 +234,29 @@ class Batch:
         f = np.ascontiguousarray(f, dtype=np.float64)
         h = np.ascontiguousarray(h, dtype=np.float64)
         N.check(N.lib().lbm_batch_set_dist(self._h, int(s), _d(f), _d(h)), "lbm_batch_set_dist")
+
+    def set_macro_ptr(self, s, rho, ux, uy, T):
+        """Equilibrium restart from host fields given as raw addresses (for
+        pinned buffers); asynchronous on the batch's stream."""
+        c = C.cast
+        N.check(N.lib().lbm_batch_set_macro(self._h, int(s), c(rho, _dp), c(ux, _dp), c(uy, _dp), c(T, _dp)),
+                "lbm_batch_set_macro")
+
+    def macro_ptr(self, s, rho, ux, uy, T, p):
+        """Macroscopic fields into host buffers given as raw addresses."""
+        c = C.cast
+        N.check(N.lib().lbm_batch_get_macro(self._h, int(s), c(rho, _dp), c(ux, _dp), c(uy, _dp), c(T, _dp),
+                                            c(p, _dp)), "lbm_batch_get_macro")
+
+    def set_macro(self, s, rho, ux, uy, T):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (rho, ux, uy, T)]
+        N.check(N.lib().lbm_batch_set_macro(self._h, int(s), *[_d(a) for a in arrs]), "lbm_batch_set_macro")
+        self.status()  # synchronises: the host arrays may be released after return
+
+    def profile(self, n=3):
+        ms = np.zeros(6)
+        N.check(N.lib().lbm_batch_profile(self._h, int(n), _d(ms), 6), "lbm_batch_profile")
+        return ms
+
+    def launches_per_step(self, residual=False):
+        return N.lib().lbm_batch_launches_per_step(self._h, 1 if residual else 0)
