@@ -39,6 +39,10 @@ struct SampleParams {
     long long node_off;  // offset into per-node arrays
     int xoff, yoff;      // offsets into the per-column / per-row spacing tables
     double R, bR, K, Tc, inv_sRTc, RTc, mu, Pr, dt, c;
+    // Reference rest state of the stored deviations (mixed path): the state
+    // holds f - f_ref, h - h_ref with f_ref, h_ref the equilibria at
+    // (rho0, 0, 0, T0); rho0 = shref = 0 (full storage) on the FP64 path.
+    double rho0, T0n, shref;  // T0n = T0 / Tc
 };
 
 struct Tile {
@@ -175,6 +179,166 @@ __device__ __forceinline__ void eq_fam9(const EqState<C> &q, C *f, C *h)
     }
 }
 
+// ------------------------------------------------ equilibria as deviations
+// The same polynomials as deviations from the rest state (rho0, 0, 0, T0)
+// of the sample, for the FP32 path: f_eq - f_ref = rho dP + (rho - rho0) P0
+// where dP = P(u, v, T) - P(0, 0, T0) keeps only terms that vanish at rest:
+// the T-only part g(T) - g(T0) is factored as (T - T0) G(T, T0), so no
+// O(1) terms cancel in FP32.  Likewise for h with the factor R Tc.
+template <class C>
+struct EqDev {
+    C rho, drho, u, v, T, tau, T0, K, RTc;
+};
+
+template <class C>
+__device__ __forceinline__ EqDev<C> eq_dev(double rho, double ux, double uy, double T, const SampleParams &sp)
+{
+    EqDev<C> e;
+    e.rho = (C)rho;
+    e.drho = (C)(rho - sp.rho0);
+    e.u = (C)(ux * sp.inv_sRTc);
+    e.v = (C)(uy * sp.inv_sRTc);
+    const double Tn = T / sp.Tc;
+    e.T = (C)Tn;
+    e.tau = (C)(Tn - sp.T0n);
+    e.T0 = (C)sp.T0n;
+    e.K = (C)sp.K;
+    e.RTc = (C)sp.RTc;
+    return e;
+}
+
+template <class C>
+__device__ __forceinline__ void eqd_fam0(const EqDev<C> &q, C &f0, C &h0)
+{
+    const C a = q.u * q.u, c = q.v * q.v, s2 = a + c, pc = a * c, T = q.T, T2 = T * T, K = q.K, T0 = q.T0;
+    const C S2 = T + T0, S3 = T2 + T * T0 + T0 * T0;
+    const C dP = C(2.5) * T * s2 + C(0.25) * (a * a + c * c) + pc - C(1.25) * s2 + q.tau * (C(2.5) * S2 - C(2.5));
+    const C P0 = C(1) + C(2.5) * T0 * T0 - C(2.5) * T0;
+    f0 = q.rho * dP + q.drho * P0;
+    const C dQ = T2 * (C(1.25) * K + C(11.25)) * s2
+                 + T * (C(0.125) * K * (s2 * s2 + C(2) * pc) - C(0.625) * K * s2 + C(2.5) * s2 * s2 + C(2.5) * pc - C(5) * s2)
+                 + s2 * s2 * s2 * C(0.125) + C(0.25) * pc * s2 - C(0.625) * s2 * s2 + C(0.5) * s2
+                 + q.tau * ((C(1.25) * K + C(20.0 / 3.0)) * S3 + (C(-1.25) * K - C(5)) * S2 + C(0.5) * K + C(1));
+    const C Q0 = T0 * T0 * T0 * (C(1.25) * K + C(20.0 / 3.0)) + T0 * T0 * (C(-1.25) * K - C(5)) + T0 * (C(0.5) * K + C(1));
+    h0 = q.RTc * (q.rho * dQ + q.drho * Q0);
+}
+
+template <class C>
+__device__ __forceinline__ void eqd_fam1(const EqDev<C> &q, C *f, C *h)
+{
+    const C T = q.T, T2 = T * T, K = q.K, T0 = q.T0;
+    const C S2 = T + T0, S3 = T2 + T * T0 + T0 * T0;
+    const C P0 = -T0 * T0 + C(2.0 / 3.0) * T0;
+    const C Q0 = T0 * T0 * T0 * (C(-0.5) * K - C(8.0 / 3.0)) + T0 * T0 * (K * C(1.0 / 3.0) + C(4.0 / 3.0));
+    const C Gf = -S2 + C(2.0 / 3.0);
+    const C Gh = (C(-0.5) * K - C(8.0 / 3.0)) * S3 + (K * C(1.0 / 3.0) + C(4.0 / 3.0)) * S2;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const C U = k == 0 ? q.u : q.v;
+        const C W = k == 0 ? q.v : q.u;
+        const C A = U * U, Cc = W * W;
+        C E = T * (C(-1.5) * A - C(0.5) * Cc) + C(2.0 / 3.0) * A - A * A * C(1.0 / 6.0) - C(0.5) * A * Cc + q.tau * Gf;
+        C O = U * (C(2.0 / 3.0) - T - A * C(1.0 / 6.0) - C(0.5) * Cc);
+        f[k] = q.rho * (E + O) + q.drho * P0;
+        f[k + 2] = q.rho * (E - O) + q.drho * P0;
+        E = T2 * (-(C(0.75) * K + C(6.5)) * A - (C(0.25) * K + C(2.5)) * Cc)
+            + T * (-(K * C(1.0 / 12.0) + C(19.0 / 12.0)) * A * A - (C(0.25) * K + C(3.5)) * A * Cc
+                   + (K * C(1.0 / 3.0) + C(7.0 / 3.0)) * A - C(0.25) * Cc * Cc + Cc * C(1.0 / 3.0))
+            - A * A * A * C(1.0 / 12.0) - A * A * Cc * C(1.0 / 3.0) + A * A * C(1.0 / 3.0) - C(0.25) * A * Cc * Cc
+            + A * Cc * C(1.0 / 3.0) + q.tau * Gh;
+        O = U * (T2 * (C(-0.5) * K - C(3))
+                 + T * (-(K * C(1.0 / 12.0) + C(7.0 / 6.0)) * A - (C(0.25) * K + C(2.5)) * Cc + K * C(1.0 / 3.0) + C(4.0 / 3.0))
+                 - A * A * C(1.0 / 12.0) - A * Cc * C(1.0 / 3.0) + A * C(1.0 / 3.0) - C(0.25) * Cc * Cc + Cc * C(1.0 / 3.0));
+        h[k] = q.RTc * (q.rho * (E + O) + q.drho * Q0);
+        h[k + 2] = q.RTc * (q.rho * (E - O) + q.drho * Q0);
+    }
+}
+
+template <class C>
+__device__ __forceinline__ void eqd_fam5(const EqDev<C> &q, C *f, C *h)
+{
+    const C u = q.u, v = q.v, a = u * u, c = v * v, s2 = a + c, pc = a * c, T = q.T, T2 = T * T, K = q.K, T0 = q.T0;
+    const C S2 = T + T0, S3 = T2 + T * T0 + T0 * T0;
+    const C P0 = C(0.25) * T0 * T0;
+    const C base = C(0.25) * q.tau * S2;
+    const C Ap = a + u, Am = a - u, Bp = c + v, Bm = c - v;
+    f[0] = q.rho * (base + C(0.25) * (T * (Ap + Bp) + Ap * Bp)) + q.drho * P0;
+    f[1] = q.rho * (base + C(0.25) * (T * (Am + Bp) + Am * Bp)) + q.drho * P0;
+    f[2] = q.rho * (base + C(0.25) * (T * (Am + Bm) + Am * Bm)) + q.drho * P0;
+    f[3] = q.rho * (base + C(0.25) * (T * (Ap + Bm) + Ap * Bm)) + q.drho * P0;
+    const C k8 = C(0.125) * K;
+    const C Q0 = T0 * T0 * T0 * (k8 + C(2.0 / 3.0));
+    const C EE = T2 * (k8 + C(1.125)) * s2 + T * ((k8 + C(1.5)) * pc + C(0.125) * (a * a + c * c)) + C(0.125) * pc * s2
+                 + q.tau * (k8 + C(2.0 / 3.0)) * S3;
+    const C OE = u * (T2 * (k8 + C(0.75)) + T * ((k8 + C(1.125)) * c + C(0.125) * a) + C(0.125) * c * s2);
+    const C EO = v * (T2 * (k8 + C(0.75)) + T * ((k8 + C(1.125)) * a + C(0.125) * c) + C(0.125) * a * s2);
+    const C OO = u * v * (T * (k8 + C(0.75)) + C(0.125) * s2);
+    h[0] = q.RTc * (q.rho * (EE + OE + EO + OO) + q.drho * Q0);
+    h[1] = q.RTc * (q.rho * (EE - OE + EO - OO) + q.drho * Q0);
+    h[2] = q.RTc * (q.rho * (EE - OE - EO + OO) + q.drho * Q0);
+    h[3] = q.RTc * (q.rho * (EE + OE - EO - OO) + q.drho * Q0);
+}
+
+template <class C>
+__device__ __forceinline__ void eqd_fam9(const EqDev<C> &q, C *f, C *h)
+{
+    const C T = q.T, T2 = T * T, K = q.K, T0 = q.T0;
+    const C S2 = T + T0, S3 = T2 + T * T0 + T0 * T0;
+    const C P0 = C(0.125) * T0 * T0 - T0 * C(1.0 / 24.0);
+    const C Q0 = T0 * T0 * T0 * (K * C(1.0 / 16.0) + C(1.0 / 3.0)) + T0 * T0 * (-K * C(1.0 / 48.0) - C(1.0 / 12.0));
+    const C Gf = S2 * C(0.125) - C(1.0 / 24.0);
+    const C Gh = (K * C(1.0 / 16.0) + C(1.0 / 3.0)) * S3 + (-K * C(1.0 / 48.0) - C(1.0 / 12.0)) * S2;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const C U = k == 0 ? q.u : q.v;
+        const C W = k == 0 ? q.v : q.u;
+        const C A = U * U, Cc = W * W;
+        C E = T * A * C(0.25) + (A * A - A) * C(1.0 / 24.0) + q.tau * Gf;
+        C O = U * (C(0.25) * T + (A - C(1)) * C(1.0 / 12.0));
+        f[k] = q.rho * (E + O) + q.drho * P0;
+        f[k + 2] = q.rho * (E - O) + q.drho * P0;
+        E = T2 * ((C(0.125) * K + C(17.0 / 16.0)) * A + Cc * C(1.0 / 16.0))
+            + T * ((K * C(1.0 / 48.0) + C(1.0 / 3.0)) * A * A - (K * C(1.0 / 48.0) + C(7.0 / 48.0)) * A + C(0.125) * A * Cc
+                   - Cc * C(1.0 / 48.0))
+            + (A * A * A + A * A * Cc - A * A - A * Cc) * C(1.0 / 48.0) + q.tau * Gh;
+        O = U * (T2 * (C(0.125) * K + C(0.75)) + T * ((K * C(1.0 / 24.0) + C(11.0 / 24.0)) * A - K * C(1.0 / 24.0) - C(1.0 / 6.0) + C(0.125) * Cc)
+                 + (A * A + A * Cc - A - Cc) * C(1.0 / 24.0));
+        h[k] = q.RTc * (q.rho * (E + O) + q.drho * Q0);
+        h[k + 2] = q.RTc * (q.rho * (E - O) + q.drho * Q0);
+    }
+}
+
+// Equilibria of one family in the stored representation: full values on the
+// FP64 path, deviations from the rest state on the FP32 path.
+template <class C, bool DEV>
+struct EqArgs;
+template <class C>
+struct EqArgs<C, false> {
+    EqState<C> q;
+    __device__ __forceinline__ EqArgs(double rho, double ux, double uy, double T, const SampleParams &sp)
+        : q(eq_state<C>(rho, ux, uy, T, sp)) {}
+    __device__ __forceinline__ void fam(int f, C *fe, C *he) const
+    {
+        if (f == 0) eq_fam0(q, fe[0], he[0]);
+        else if (f == 1) eq_fam1(q, fe, he);
+        else if (f == 2) eq_fam5(q, fe, he);
+        else eq_fam9(q, fe, he);
+    }
+};
+template <class C>
+struct EqArgs<C, true> {
+    EqDev<C> q;
+    __device__ __forceinline__ EqArgs(double rho, double ux, double uy, double T, const SampleParams &sp)
+        : q(eq_dev<C>(rho, ux, uy, T, sp)) {}
+    __device__ __forceinline__ void fam(int f, C *fe, C *he) const
+    {
+        if (f == 0) eqd_fam0(q, fe[0], he[0]);
+        else if (f == 1) eqd_fam1(q, fe, he);
+        else if (f == 2) eqd_fam5(q, fe, he);
+        else eqd_fam9(q, fe, he);
+    }
+};
+
 // all 26 values (init, pointwise stages)
 template <class C>
 __device__ __forceinline__ void eq_all(const EqState<C> &q, C *f, C *h)
@@ -195,6 +359,10 @@ struct Macro {
 
 __device__ __forceinline__ Macro macro_from_sums(double r, double rux, double ruy, double sh, const SampleParams &sp)
 {
+    // stored deviations: add the rest state's rho0 and sum of h (0 when the
+    // state is stored in full)
+    r = sp.rho0 + r;
+    sh = sp.shref + sh;
     Macro m;
     m.rho = r;
     m.ux = rux / r;

@@ -72,6 +72,7 @@ struct HostSample {
     int nx = 0, ny = 0, rk = 1, fm = 1;
     int flags = 0;
     double R = 1, b = 5, K = 3, Tc = 1, c = 1, mu = 0, Pr = 1, dt = 0, tol = 0;
+    double rho_ref = 1, T_ref = 1;  // completed reference state (refineInput)
     int nsteps = 0;
     std::vector<double> dx, dy;
     std::vector<uint8_t> type;  // [y*nx + x]
@@ -142,6 +143,8 @@ static HostSample derive(const lbm_config &c, const lbm_init &in)
         s.dy[y] = c.dy_array ? c.dy_array[y] : dy;
         if (nonuni) mind = std::min(mind, s.dy[y]);
     }
+    s.rho_ref = rho_ref;
+    s.T_ref = T_ref;
     s.b = 2 / (c.gamma - 1);
     s.K = s.b - 2;
     s.Tc = c.Tc_Tref * T_ref;
@@ -238,6 +241,7 @@ struct lbm_batch {
     DevBuf<Tile> d_tiles_by_rk[4];
     DevBuf<WallNode> d_walls_all, d_walls_rk3;
     DevBuf<CUtensorMap> d_maps;
+    DevBuf<double> d_fref;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // [want_residual]
     std::vector<int> host_status;
     std::vector<double> host_residual;
@@ -273,6 +277,7 @@ struct lbm_batch {
         a.dxv = dxv.p;
         a.dyv = dyv.p;
         a.tmaps = d_maps.p;
+        a.fref = d_fref.p;
         a.want_residual = want_res;
         a.eq_tol = 1e-6;
         return a;
@@ -297,7 +302,7 @@ struct lbm_batch {
         CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 
         // layout: per sample 26 planes of ny x pitch, pitch a multiple of 32
-        std::vector<double> v_tdx, v_tdy, v_dx, v_dy;
+        std::vector<double> v_tdx, v_tdy, v_dx, v_dy, fref_host;
         std::vector<uint8_t> flags;
         long long state_off = 0, node_off = 0;
         for (int k = 0; k < n; ++k) {
@@ -324,6 +329,36 @@ struct lbm_batch {
             p.Pr = h.Pr;
             p.dt = h.dt;
             p.c = h.c;
+            // rest state of the stored deviations (FP32 path only)
+            if (prec == LBM_PREC_F32) {
+                p.rho0 = (h.rho_ref > 0 && std::isfinite(h.rho_ref)) ? h.rho_ref : 1.0;
+                p.T0n = (h.T_ref > 0 && std::isfinite(h.T_ref)) ? h.T_ref / h.Tc : 1.0;
+            } else {
+                p.rho0 = 0.0;
+                p.T0n = 1.0;
+            }
+            {
+                // equilibria at rest per family (the polynomials at u = v = 0)
+                const double T = p.T0n, K = h.K;
+                const double P0[4] = {1 + 2.5 * T * T - 2.5 * T, -T * T + 2.0 * T / 3.0, 0.25 * T * T,
+                                      0.125 * T * T - T / 24.0};
+                const double Q0[4] = {T * T * T * (1.25 * K + 20.0 / 3.0) + T * T * (-1.25 * K - 5) + T * (0.5 * K + 1),
+                                      T * T * T * (-0.5 * K - 8.0 / 3.0) + T * T * (K / 3.0 + 4.0 / 3.0),
+                                      T * T * T * (K / 8.0 + 2.0 / 3.0),
+                                      T * T * T * (K / 16.0 + 1.0 / 3.0) + T * T * (-K / 48.0 - 1.0 / 12.0)};
+                double sh = 0;
+                for (int i = 0; i < NQ; ++i) {
+                    const int fam = i == 0 ? 0 : (i <= 4 ? 1 : (i <= 8 ? 2 : 3));
+                    fref_host.push_back(p.rho0 * P0[fam]);
+                }
+                for (int i = 0; i < NQ; ++i) {
+                    const int fam = i == 0 ? 0 : (i <= 4 ? 1 : (i <= 8 ? 2 : 3));
+                    const double hv = p.rho0 * h.R * h.Tc * Q0[fam];
+                    fref_host.push_back(hv);
+                    sh += hv;
+                }
+                p.shref = sh;
+            }
             for (int x = 0; x < h.nx; ++x) { v_tdx.push_back(h.dt / h.dx[x]); v_dx.push_back(h.dx[x]); }
             for (int y = 0; y < h.ny; ++y) { v_tdy.push_back(h.dt / h.dy[y]); v_dy.push_back(h.dy[y]); }
             state_off += NPL * p.plane;
@@ -399,6 +434,7 @@ struct lbm_batch {
         dxv.upload(v_dx, stream);
         dyv.upload(v_dy, stream);
         d_sp.upload(sp, stream);
+        d_fref.upload(fref_host, stream);
         d_tiles_all.upload(tiles_all, stream);
         d_tiles_rk3.upload(tiles_rk3, stream);
         for (int m = 0; m < 4; ++m) d_tiles_by_rk[m].upload(tiles_by_rk[m], stream);
@@ -533,10 +569,10 @@ struct lbm_batch {
             CU(cudaMemcpyAsync(scratch.p + k * n, src[k], n * sizeof(double), cudaMemcpyHostToDevice, stream));
         if (prec == LBM_PREC_F64)
             CU(launch_set_macro<double>(d_sp.p, s, reinterpret_cast<double *>(state.p), reinterpret_cast<double *>(buf2.p),
-                                        reinterpret_cast<double *>(buf3.p), scratch.p, nflags.p, n, stream));
+                                        reinterpret_cast<double *>(buf3.p), scratch.p, nflags.p, d_fref.p, n, stream));
         else
             CU(launch_set_macro<float>(d_sp.p, s, reinterpret_cast<float *>(state.p), reinterpret_cast<float *>(buf2.p),
-                                       reinterpret_cast<float *>(buf3.p), scratch.p, nflags.p, n, stream));
+                                       reinterpret_cast<float *>(buf3.p), scratch.p, nflags.p, d_fref.p, n, stream));
     }
 
     void enqueue_step(int want_res)
@@ -616,10 +652,12 @@ struct lbm_batch {
         }
         if (prec == LBM_PREC_F64)
             CU(launch_dist_io<double>(d_sp.p, s, reinterpret_cast<double *>(state.p), reinterpret_cast<double *>(buf2.p),
-                                      reinterpret_cast<double *>(buf3.p), scratch.p, to_aos ? 1 : 0, nflags.p, n, stream));
+                                      reinterpret_cast<double *>(buf3.p), scratch.p, to_aos ? 1 : 0, nflags.p, d_fref.p, n,
+                                      stream));
         else
             CU(launch_dist_io<float>(d_sp.p, s, reinterpret_cast<float *>(state.p), reinterpret_cast<float *>(buf2.p),
-                                     reinterpret_cast<float *>(buf3.p), scratch.p, to_aos ? 1 : 0, nflags.p, n, stream));
+                                     reinterpret_cast<float *>(buf3.p), scratch.p, to_aos ? 1 : 0, nflags.p, d_fref.p, n,
+                                     stream));
         if (to_aos) {
             if (f) CU(cudaMemcpyAsync(f, scratch.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
             if (h) CU(cudaMemcpyAsync(h, scratch.p + n3, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream));

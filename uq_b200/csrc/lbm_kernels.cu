@@ -49,14 +49,16 @@ __global__ void k_init(KArgs<S> a, const double *__restrict__ rho, const double 
     if (fabs(sf - rho[node]) > 1e-6) atomicOr(&a.status[t.sample], STATUS_EQ);
     const bool fixed = (a.nflags[node] & NF_TYPE) != 0;
     const long long o = (long long)y * sp.pitch + x;
+    const double *fr = a.fref + NPL * t.sample;
     for (int i = 0; i < NQ; ++i) {
-        plane_ptr(a.state, sp, i)[o] = (S)f[i];
-        plane_ptr(a.state, sp, NQ + i)[o] = (S)h[i];
+        const S fv = (S)(f[i] - fr[i]), hv = (S)(h[i] - fr[NQ + i]);
+        plane_ptr(a.state, sp, i)[o] = fv;
+        plane_ptr(a.state, sp, NQ + i)[o] = hv;
         if (fixed) {
-            plane_ptr(a.buf2, sp, i)[o] = (S)f[i];
-            plane_ptr(a.buf2, sp, NQ + i)[o] = (S)h[i];
-            plane_ptr(a.buf3, sp, i)[o] = (S)f[i];
-            plane_ptr(a.buf3, sp, NQ + i)[o] = (S)h[i];
+            plane_ptr(a.buf2, sp, i)[o] = fv;
+            plane_ptr(a.buf2, sp, NQ + i)[o] = hv;
+            plane_ptr(a.buf3, sp, i)[o] = fv;
+            plane_ptr(a.buf3, sp, NQ + i)[o] = hv;
         }
     }
 }
@@ -89,8 +91,8 @@ __global__ void __launch_bounds__(256, 2) k_stage0(KArgs<S> a)
     const long long o = (long long)y * sp.pitch + x;
     const long long node = sp.node_off + o;
     const int type = a.nflags[node] & NF_TYPE;
-    const S *st = a.state + sp.state_off;
-    S *b2 = a.buf2 + sp.state_off;
+    const S *__restrict__ st = a.state + sp.state_off;
+    S *__restrict__ b2 = a.buf2 + sp.state_off;
     if (RK >= 2) {  // EULER, EULER_EQ: fluxes of the state itself
         if (type == 0)
             for (int p = 0; p < NPL; ++p) b2[(long long)p * sp.plane + o] = st[(long long)p * sp.plane + o];
@@ -100,14 +102,19 @@ __global__ void __launch_bounds__(256, 2) k_stage0(KArgs<S> a)
     if (type != 0) return;
     const Macro m = node_macro(st, sp, o);
     if (a.want_residual) a.told[node] = m.T;
-    const EqState<C> q = eq_state<C>(m.rho, m.ux, m.uy, m.T, sp);
+    constexpr bool DEV = sizeof(S) == 4;
+    const EqArgs<C, DEV> q(m.rho, m.ux, m.uy, m.T, sp);
     C fe[NQ], he[NQ];
-    eq_all(q, fe, he);
+    q.fam(0, fe, he);
+    q.fam(1, fe + 1, he + 1);
+    q.fam(2, fe + 5, he + 5);
+    q.fam(3, fe + 9, he + 9);
     {
+        // sum_i f_eq = rho (the stored values: sum = rho - rho0)
         double sf = 0;
 #pragma unroll
         for (int i = 0; i < NQ; ++i) sf += (double)fe[i];
-        if (fabs(sf - m.rho) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(m.rho))))
+        if (fabs(sf - (m.rho - sp.rho0)) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(m.rho))))
             atomicOr(&a.status[t.sample], STATUS_EQ);
     }
     const C dt = (C)sp.dt, ux = (C)m.ux, uy = (C)m.uy;
@@ -161,6 +168,7 @@ __global__ void k_wall(KArgs<S> a, const S *__restrict__ stage, const WallNode *
     const SampleParams sp = a.samples[w.sample];
     const StageView<S> v{stage + sp.state_off, a.nflags + sp.node_off, (int)sp.plane, sp.pitch};
     const double dxm = a.dxv[sp.xoff + w.x], dym = a.dyv[sp.yoff + w.y];
+    const double *fr = a.fref + NPL * w.sample;  // stored values + fr = full values
     double fin = 0, fout = 0;
     for (int j = 0; j < 4; ++j) {
         int m;
@@ -172,13 +180,14 @@ __global__ void k_wall(KArgs<S> a, const S *__restrict__ stage, const WallNode *
         const double dd = axis == 0 ? dxm : dym;
         for (int q = 0; q < 4; ++q) {
             const int i = c_WII[j][q], io = c_WINV[j][q];
-            const double F = (double)flux_axis<S, C>(sp, v, xm, ym, i, axis, fl);
+            const double ai = sp.c * abs(axis == 0 ? c_EX[i] : c_EY[i]);
+            const double F = (double)flux_axis<S, C>(sp, v, xm, ym, i, axis, fl) + ai * fr[i];
             fin += F / dd;
-            const double fo = (double)ldv(v, io, w.x, w.y);
+            const double fo = (double)ldv(v, io, w.x, w.y) + fr[io];
             fout += fo * (sp.c * abs(axis == 0 ? c_EX[io] : c_EY[io])) / dd;
         }
     }
-    a.template alpha_as<C>()[sp.node_off + (long long)w.y * sp.pitch + w.x] = (C)(fin / fout);
+    a.template alpha_as<C>()[sp.node_off + (long long)w.y * sp.pitch + w.x] = (C)(fin / fout - 1.0);
 }
 
 // ------------------------------------------------------------------ P1/P2
@@ -224,7 +233,8 @@ template <class S, class C>
 struct TileCtx {
     const SampleParams *sp;
     StageView<S> v;
-    const C *alpha;  // alpha of this sample (node-indexed)
+    const C *alpha;  // alpha - 1 of this sample (node-indexed)
+    const double *fref;  // this sample's 26 rest-state values
     C *sf;           // [2 buffers][4: fx_f, fx_h, fy_f, fy_h][NT]
     C *ringx;        // [2 buffers][2: f, h][TY]
     C *ringy;        // [2 buffers][2: f, h][TX]
@@ -276,7 +286,12 @@ __device__ __forceinline__ C any_node_flux(TileCtx<S, C> &k, const S *box, int i
     const int oo = yn * k.v.pitch + xn;
     const uint8_t fl = k.v.nf[oo];
     const C ae = (C)(sp.c * (double)abs(ev));
-    if ((fl & NF_TYPE) == 2) return k.alpha[oo] * ae * (C)__ldg(k.v.st + (pp * k.v.plane + oo));
+    if ((fl & NF_TYPE) == 2) {
+        // wallFluxes' alpha |e| f on full values, written for stored ones:
+        // |e| (f_s + (alpha - 1)(f_s + f_ref)) - |e| f_ref
+        const C fs = (C)__ldg(k.v.st + (pp * k.v.plane + oo));
+        return ae * (fs + k.alpha[oo] * (fs + (C)k.fref[pp]));
+    }
     const uint8_t edge = axis == 0 ? (NF_SOLX | NF_EDGX | NF_WRPX) : (NF_SOLY | NF_EDGY | NF_WRPY);
     if (in_box && !mirrored && !(fl & edge)) {
         const int lx = xn - (k.x0 - HALO_X), ly = yn - (k.y0 - HALO_Y);
@@ -321,10 +336,12 @@ __device__ __forceinline__ void dir_step(TileCtx<S, C> &k, const int i)
         const S *cf = box + ly * k.BW + lx;
         const S *ch = cf + k.pstride;
         if (type == 2) {
-            const C al = k.alpha[k.o];
+            // alpha |e| f of wallFluxes on stored deviations (see any_node_flux)
+            const C am1 = k.alpha[k.o];
             const C fv = (C)cf[0], hv = (C)ch[0];
-            if (SX) { sf[k.tid] = al * aex * fv; sf[NT + k.tid] = al * aex * hv; }
-            if (SY) { sf[2 * NT + k.tid] = al * aey * fv; sf[3 * NT + k.tid] = al * aey * hv; }
+            const C gf = fv + am1 * (fv + (C)k.fref[i]), gh = hv + am1 * (hv + (C)k.fref[NQ + i]);
+            if (SX) { sf[k.tid] = aex * gf; sf[NT + k.tid] = aex * gh; }
+            if (SY) { sf[2 * NT + k.tid] = aey * gf; sf[3 * NT + k.tid] = aey * gh; }
         } else {
             if (SX) {
                 C a, b;
@@ -474,6 +491,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     k.sp = &sp;
     k.v = v;
     k.alpha = alpha;
+    k.fref = a.fref + NPL * t.sample;
     k.sf = sf;
     k.ringx = ringx;
     k.ringy = ringy;
@@ -493,9 +511,9 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
 
     double res_part = 0;
     if (active && type == 0) {
-        S *st = a.state + sp.state_off;
-        const S *b2 = a.buf2 + sp.state_off;
-        S *b3 = a.buf3 + sp.state_off;
+        S *__restrict__ st = a.state + sp.state_off;
+        const S *__restrict__ b2 = a.buf2 + sp.state_off;
+        S *__restrict__ b3 = a.buf3 + sp.state_off;
         const C dt = (C)sp.dt;
         bool final_phase = true;
         if (MODE == 1) {
@@ -504,12 +522,12 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             final_phase = false;
             // stage-1 moments (= stage 2's) and the moments of f - div F(f2)
             // (macroProp3, cpuLBM.cpp:973-1032), both summed in FP64
-            EqState<C> q1, q3;
+            constexpr bool DEV = sizeof(S) == 4;
+            Macro m1, m3;
             C tf2, th2, thf2, tf3, th3, thf3, ux1, uy1, ux3, uy3;
             double rho3;
             {
-                const Macro m1 = node_macro(st, sp, o);
-                q1 = eq_state<C>(m1.rho, m1.ux, m1.uy, m1.T, sp);
+                m1 = node_macro(st, sp, o);
                 tf2 = (C)m1.tf; th2 = (C)m1.th; thf2 = (C)m1.thf; ux1 = (C)m1.ux; uy1 = (C)m1.uy;
             }
             {
@@ -523,11 +541,12 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     ruy += fv * (sp.c * c_EY[i]) - Df * (sp.c * c_EY[i]);
                     sh += (double)st[(long long)(NQ + i) * sp.plane + o] - (double)sD[(NQ + i) * NT + tid];
                 }
-                const Macro m3 = macro_from_sums(r, rux, ruy, sh, sp);
-                q3 = eq_state<C>(m3.rho, m3.ux, m3.uy, m3.T, sp);
+                m3 = macro_from_sums(r, rux, ruy, sh, sp);
                 tf3 = (C)m3.tf; th3 = (C)m3.th; thf3 = (C)m3.thf; ux3 = (C)m3.ux; uy3 = (C)m3.uy;
                 rho3 = m3.rho;
             }
+            const EqArgs<C, DEV> q1(m1.rho, m1.ux, m1.uy, m1.T, sp);
+            const EqArgs<C, DEV> q3(m3.rho, m3.ux, m3.uy, m3.T, sp);
             const C hdt = dt * C(0.5);
             const C a2 = hdt / tf2, a3 = hdt / tf3, b2c = hdt / th2, b3c = hdt / th3;
             const C ia3 = C(1) / (C(1) + a3), ib3 = C(1) / (C(1) + b3c);
@@ -537,18 +556,23 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
 #pragma unroll 1
             for (int fam = 0; fam < 4; ++fam) {
                 C e1f[4], e1h[4], e3f[4], e3h[4];
-                int i0, n;
-                if (fam == 0) { eq_fam0(q1, e1f[0], e1h[0]); eq_fam0(q3, e3f[0], e3h[0]); i0 = 0; n = 1; }
-                else if (fam == 1) { eq_fam1(q1, e1f, e1h); eq_fam1(q3, e3f, e3h); i0 = 1; n = 4; }
-                else if (fam == 2) { eq_fam5(q1, e1f, e1h); eq_fam5(q3, e3f, e3h); i0 = 5; n = 4; }
-                else { eq_fam9(q1, e1f, e1h); eq_fam9(q3, e3f, e3h); i0 = 9; n = 4; }
+                q1.fam(fam, e1f, e1h);
+                q3.fam(fam, e3f, e3h);
+                const int i0 = fam == 0 ? 0 : 4 * fam - 3, n = fam == 0 ? 1 : 4;
+                C vf[4], vh[4], vf2[4], vh2[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (k >= n) break;
+                    const long long of = (long long)(i0 + k) * sp.plane + o, oh = (long long)(NQ + i0 + k) * sp.plane + o;
+                    vf[k] = (C)st[of]; vh[k] = (C)st[oh]; vf2[k] = (C)b2[of]; vh2[k] = (C)b2[oh];
+                }
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if (k >= n) break;
                     const int i = i0 + k;
                     sf3 += (double)e3f[k];
                     const long long of = (long long)i * sp.plane + o, oh = (long long)(NQ + i) * sp.plane + o;
-                    const C f = (C)st[of], h = (C)st[oh], f2 = (C)b2[of], h2 = (C)b2[oh];
+                    const C f = vf[k], h = vh[k], f2 = vf2[k], h2 = vh2[k];
                     const C Df = sD[i * NT + tid], Dh = sD[(NQ + i) * NT + tid];
                     const C exi = (C)(sp.c * c_EX[i]), eyi = (C)(sp.c * c_EY[i]);
                     const C eu2 = exi * ux1 + eyi * uy1, eu3 = exi * ux3 + eyi * uy3;
@@ -565,40 +589,49 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     st[oh] = (S)acch;
                 }
             }
-            if (fabs(sf3 - rho3) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(rho3))))
+            if (fabs(sf3 - (rho3 - sp.rho0)) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(rho3))))
                 atomicOr(&a.status[t.sample], STATUS_EQ);
         } else if (MODE == 2) {
-            // final RK3 combination (cpuLBM.cpp:1999-2042): f = acc - D3/2
-            for (int p = 0; p < NPL; ++p) {
-                const long long op = (long long)p * sp.plane + o;
-                st[op] = (S)((C)st[op] - C(0.5) * sD[p * NT + tid]);
-            }
+            // final RK3 combination (cpuLBM.cpp:1999-2042): f = acc - D3/2;
+            // all loads first, then the stores (no load waits behind a store)
+            S acc[NPL];
+#pragma unroll
+            for (int p = 0; p < NPL; ++p) acc[p] = st[(long long)p * sp.plane + o];
+#pragma unroll
+            for (int p = 0; p < NPL; ++p)
+                st[(long long)p * sp.plane + o] = (S)((C)acc[p] - C(0.5) * sD[p * NT + tid]);
         } else {
             // RK1 update (cpuLBM.cpp:1674-1710), EULER (:2130-2168), EULER_EQ (:2220-2258)
             const Macro m = node_macro(st, sp, o);
-            const EqState<C> q = eq_state<C>(m.rho, m.ux, m.uy, m.T, sp);
+            constexpr bool DEV = sizeof(S) == 4;
+            const EqArgs<C, DEV> q(m.rho, m.ux, m.uy, m.T, sp);
             const C tf = (C)m.tf, th = (C)m.th, thf = (C)m.thf, ux = (C)m.ux, uy = (C)m.uy;
             double sf = 0;
 #pragma unroll 1
             for (int fam = 0; fam < 4; ++fam) {
                 C fe[4], he[4];
-                int i0, n;
-                if (fam == 0) { eq_fam0(q, fe[0], he[0]); i0 = 0; n = 1; }
-                else if (fam == 1) { eq_fam1(q, fe, he); i0 = 1; n = 4; }
-                else if (fam == 2) { eq_fam5(q, fe, he); i0 = 5; n = 4; }
-                else { eq_fam9(q, fe, he); i0 = 9; n = 4; }
+                q.fam(fam, fe, he);
+                const int i0 = fam == 0 ? 0 : 4 * fam - 3, n = fam == 0 ? 1 : 4;
+                C vf[4], vh[4], v1f[4], v1h[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (k >= n) break;
+                    const long long of = (long long)(i0 + k) * sp.plane + o, oh = (long long)(NQ + i0 + k) * sp.plane + o;
+                    vf[k] = (C)st[of]; vh[k] = (C)st[oh];
+                    if (MODE == 3) { v1f[k] = (C)b2[of]; v1h[k] = (C)b2[oh]; }
+                }
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if (k >= n) break;
                     const int i = i0 + k;
                     sf += (double)fe[k];
                     const long long of = (long long)i * sp.plane + o, oh = (long long)(NQ + i) * sp.plane + o;
-                    const C f = (C)st[of], h = (C)st[oh];
+                    const C f = vf[k], h = vh[k];
                     const C Df = sD[i * NT + tid], Dh = sD[(NQ + i) * NT + tid];
                     const C eu = (C)(sp.c * c_EX[i]) * ux + (C)(sp.c * c_EY[i]) * uy;
                     C fn, hn;
                     if (MODE == 3) {
-                        const C f1 = (C)b2[of], h1 = (C)b2[oh];
+                        const C f1 = v1f[k], h1 = v1h[k];
                         fn = f - Df + (dt / tf) * (fe[k] - f1);
                         hn = h - Dh + (dt / th) * (he[k] - h1) - ((dt * eu) / thf) * (fe[k] - f1);
                     } else if (MODE == 4) {
@@ -612,7 +645,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     st[oh] = (S)hn;
                 }
             }
-            if (MODE >= 4 && fabs(sf - m.rho) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(m.rho))))
+            if (MODE >= 4 && fabs(sf - (m.rho - sp.rho0)) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(m.rho))))
                 atomicOr(&a.status[t.sample], STATUS_EQ);
         }
         if (final_phase) {
@@ -673,8 +706,9 @@ __global__ void k_macro_out(const SampleParams *samples, int s, const S *state, 
 // planes <-> reference AoS [(x*Ny + y)*13 + i] in FP64
 template <class S>
 __global__ void k_dist_io(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, double *aos, int to_aos,
-                          const uint8_t *nflags)
+                          const uint8_t *nflags, const double *fref)
 {
+    const double *fr = fref + NPL * s;
     const SampleParams sp = samples[s];
     const long long n = (long long)sp.nx * sp.ny * NQ;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
@@ -685,11 +719,11 @@ __global__ void k_dist_io(const SampleParams *samples, int s, S *state, S *buf2,
         S *f = state + sp.state_off + (long long)i * sp.plane + o;
         S *h = state + sp.state_off + (long long)(NQ + i) * sp.plane + o;
         if (to_aos) {
-            aos[k] = (double)*f;
-            aos[n + k] = (double)*h;
+            aos[k] = (double)*f + fr[i];
+            aos[n + k] = (double)*h + fr[NQ + i];
         } else {
-            *f = (S)aos[k];
-            *h = (S)aos[n + k];
+            *f = (S)(aos[k] - fr[i]);
+            *h = (S)(aos[n + k] - fr[NQ + i]);
             if (nflags[sp.node_off + o] & NF_TYPE) {  // fixed nodes seed the stage buffers
                 const long long of = sp.state_off + (long long)i * sp.plane + o;
                 const long long oh = sp.state_off + (long long)(NQ + i) * sp.plane + o;
@@ -703,8 +737,9 @@ __global__ void k_dist_io(const SampleParams *samples, int s, S *state, S *buf2,
 // f, h = equilibria of per-node fields given in [x*Ny + y] order (FP64)
 template <class S>
 __global__ void k_set_macro(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, const double *fields,
-                            const uint8_t *nflags)
+                            const uint8_t *nflags, const double *fref)
 {
+    const double *fr = fref + NPL * s;
     const SampleParams sp = samples[s];
     const long long n = (long long)sp.nx * sp.ny;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
@@ -717,11 +752,12 @@ __global__ void k_set_macro(const SampleParams *samples, int s, S *state, S *buf
         for (int i = 0; i < NQ; ++i) {
             const long long of = sp.state_off + (long long)i * sp.plane + o;
             const long long oh = sp.state_off + (long long)(NQ + i) * sp.plane + o;
-            state[of] = (S)f[i];
-            state[oh] = (S)h[i];
+            const S fv = (S)(f[i] - fr[i]), hv = (S)(h[i] - fr[NQ + i]);
+            state[of] = fv;
+            state[oh] = hv;
             if (fixed) {
-                buf2[of] = (S)f[i]; buf3[of] = (S)f[i];
-                buf2[oh] = (S)h[i]; buf3[oh] = (S)h[i];
+                buf2[of] = fv; buf3[of] = fv;
+                buf2[oh] = hv; buf3[oh] = hv;
             }
         }
     }
@@ -729,16 +765,16 @@ __global__ void k_set_macro(const SampleParams *samples, int s, S *state, S *buf
 
 template <class S>
 cudaError_t launch_set_macro(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, const double *fields,
-                             const uint8_t *nflags, long long nodes, cudaStream_t st)
+                             const uint8_t *nflags, const double *fref, long long nodes, cudaStream_t st)
 {
     const int blocks = (int)std::min<long long>((nodes + 255) / 256, 4096);
-    k_set_macro<S><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(samples, s, state, buf2, buf3, fields, nflags);
+    k_set_macro<S><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(samples, s, state, buf2, buf3, fields, nflags, fref);
     return cudaGetLastError();
 }
 template cudaError_t launch_set_macro<double>(const SampleParams *, int, double *, double *, double *, const double *,
-                                              const uint8_t *, long long, cudaStream_t);
+                                              const uint8_t *, const double *, long long, cudaStream_t);
 template cudaError_t launch_set_macro<float>(const SampleParams *, int, float *, float *, float *, const double *,
-                                             const uint8_t *, long long, cudaStream_t);
+                                             const uint8_t *, const double *, long long, cudaStream_t);
 
 // ----------------------------------------------------------------- launchers
 // phase: 0 pointwise stages, 1 stencil phase over buffer 2, 2 RK3 final
@@ -805,10 +841,10 @@ cudaError_t launch_macro_out(const SampleParams *samples, int s, const S *state,
 
 template <class S>
 cudaError_t launch_dist_io(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, double *aos, int to_aos,
-                           const uint8_t *nflags, long long nodes, cudaStream_t st)
+                           const uint8_t *nflags, const double *fref, long long nodes, cudaStream_t st)
 {
     const int blocks = (int)std::min<long long>((nodes * NQ + 255) / 256, 8192);
-    k_dist_io<S><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(samples, s, state, buf2, buf3, aos, to_aos, nflags);
+    k_dist_io<S><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(samples, s, state, buf2, buf3, aos, to_aos, nflags, fref);
     return cudaGetLastError();
 }
 
@@ -832,8 +868,8 @@ template cudaError_t launch_init<float>(const KArgs<float> &, const double *, co
 template cudaError_t launch_macro_out<double>(const SampleParams *, int, const double *, double *, long long, cudaStream_t);
 template cudaError_t launch_macro_out<float>(const SampleParams *, int, const float *, double *, long long, cudaStream_t);
 template cudaError_t launch_dist_io<double>(const SampleParams *, int, double *, double *, double *, double *, int,
-                                            const uint8_t *, long long, cudaStream_t);
+                                            const uint8_t *, const double *, long long, cudaStream_t);
 template cudaError_t launch_dist_io<float>(const SampleParams *, int, float *, float *, float *, double *, int,
-                                           const uint8_t *, long long, cudaStream_t);
+                                           const uint8_t *, const double *, long long, cudaStream_t);
 
 }  // namespace uqlbm

@@ -31,12 +31,13 @@ struct KArgs {
     S *buf2;     // stage buffer 2 (f1 or f2)
     S *buf3;     // stage buffer 3 (f3)
     const uint8_t *nflags;
-    void *alpha_raw;
+    void *alpha_raw;  // per node: wall correction factor alpha - 1
     double *told;     // T at the start of the step (residual)
     double *partial;  // per-tile residual partial sums
     int *status;      // per-sample status bits
     const double *tdx, *tdy, *dxv, *dyv;
     const CUtensorMap *tmaps;  // per sample: [buffer 2, buffer 3]
+    const double *fref;        // per sample: 26 rest-state values subtracted from the stored state
     int want_residual;
     double eq_tol;
 #ifdef __CUDACC__
@@ -60,10 +61,10 @@ cudaError_t launch_macro_out(const SampleParams *samples, int s, const S *state,
                              cudaStream_t st);
 template <class S>
 cudaError_t launch_dist_io(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, double *aos, int to_aos,
-                           const uint8_t *nflags, long long nodes, cudaStream_t st);
+                           const uint8_t *nflags, const double *fref, long long nodes, cudaStream_t st);
 template <class S>
 cudaError_t launch_set_macro(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, const double *fields,
-                             const uint8_t *nflags, long long nodes, cudaStream_t st);
+                             const uint8_t *nflags, const double *fref, long long nodes, cudaStream_t st);
 cudaError_t launch_residual(const SampleParams *samples, int nsamples, const double *partial, const int *tile_first,
                             const int *tile_count, double *residual, cudaStream_t st);
 
