@@ -177,6 +177,34 @@ LBM_API long long lbm_batch_nodes(lbm_batch *b);
 LBM_API void *lbm_batch_stream(lbm_batch *b);
 LBM_API void lbm_batch_destroy(lbm_batch *b);
 
+/* ------------------------------------------------- allocation-free step
+ * No counterpart in the reference.  For callers that cannot call
+ * cudaMalloc: an application that owns all device memory through its own
+ * pool or arena, or code running where device allocation is not allowed
+ * (for example while it records work for later replay).  It advances one
+ * domain n_steps steps on the FP64 path with every scratch buffer taken
+ * from a fixed array that the library reserves on each GPU it is loaded on
+ * (about 10.7 MB, held until the process exits) -- nothing is allocated.
+ *
+ *   cellType  host array [Nx*Ny], the cell type (0 fluid, 1 permanent,
+ *             2 solid) of each node in [x*Ny + y] order
+ *   d_f, d_h  device arrays [(x*Ny + y)*13 + i] (the reference's f_G, h_G
+ *             layout) holding the state; updated in place
+ *   stream    cudaStream_t to run on (NULL: the default stream); the call
+ *             returns after the stream has finished the work
+ *
+ * Limits: uniform cells only (dx_array/dy_array must be NULL) and
+ * Ny * roundup(Nx, 32) <= LBM_NOALLOC_MAX_NODES, e.g. 128 x 128; larger
+ * domains return LBM_ERR_INVALID.  The first call on a device looks up the
+ * array's device address and sets kernel attributes on that device: make
+ * that first call before any stream capture on it.  All calls share the one
+ * array and each overwrites what the previous call left in it, so calls that
+ * overlap on the GPU (other threads, other streams) race; serialise them.
+ * The equilibria of moving walls are whatever d_f, d_h hold at solid nodes. */
+#define LBM_NOALLOC_MAX_NODES 16384
+LBM_API lbm_status lbm_step_noalloc(const lbm_config *cfg, int Nx, int Ny, const int *cellType, double *d_f,
+                                    double *d_h, int n_steps, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

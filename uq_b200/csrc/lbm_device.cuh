@@ -553,4 +553,39 @@ __device__ __forceinline__ C flux_axis(const SampleParams &sp, const StageView<S
     return nnd3<C>(ae, (C)__ldg(c0 - stride), (C)__ldg(c0), (C)__ldg(c0 + stride));
 }
 
+// wallFluxes (cpuLBM.cpp:1502-1590): for a solid node next to fluid,
+// alpha = (f flux of the fluid 4-neighbours into it) / (|e| f out of it),
+// weighted by the solid cell's 1/dx, 1/dy; one alpha for f and h.  Works on
+// full values (stored values + fr, the rest state of stored deviations) and
+// returns alpha - 1.
+__constant__ int c_WXX[4] = {-1, 1, 0, 0};
+__constant__ int c_WYY[4] = {0, 0, -1, 1};
+__constant__ int c_WII[4][4] = {{1, 5, 8, 9}, {3, 6, 7, 11}, {2, 5, 6, 10}, {4, 7, 8, 12}};
+__constant__ int c_WINV[4][4] = {{3, 6, 7, 11}, {1, 5, 8, 9}, {4, 8, 7, 12}, {2, 6, 5, 10}};
+
+template <class S, class C>
+__device__ double wall_alpha_m1(const SampleParams &sp, const StageView<S> &v, int x, int y, double dxm, double dym,
+                                const double *fr)
+{
+    double fin = 0, fout = 0;
+    for (int j = 0; j < 4; ++j) {
+        int m;
+        const int xm = bc_index(sp, x, c_WXX[j], 0, m);
+        const int ym = bc_index(sp, y, c_WYY[j], 1, m);
+        const uint8_t fl = v.nf[ym * v.pitch + xm];
+        if ((fl & NF_TYPE) >= 2) continue;
+        const int axis = j < 2 ? 0 : 1;
+        const double dd = axis == 0 ? dxm : dym;
+        for (int q = 0; q < 4; ++q) {
+            const int i = c_WII[j][q], io = c_WINV[j][q];
+            const double ai = sp.c * abs(axis == 0 ? c_EX[i] : c_EY[i]);
+            const double F = (double)flux_axis<S, C>(sp, v, xm, ym, i, axis, fl) + ai * fr[i];
+            fin += F / dd;
+            const double fo = (double)ldv(v, io, x, y) + fr[io];
+            fout += fo * (sp.c * abs(axis == 0 ? c_EX[io] : c_EY[io])) / dd;
+        }
+    }
+    return fin / fout - 1.0;
+}
+
 }  // namespace uqlbm

@@ -9,6 +9,7 @@
 // follows runSimStep (main.cpp:32-112).
 #include "lbm_device.cuh"
 #include "lbm_kernels.h"
+#include "lbm_host.h"
 #include "../../include/uq_lbm.h"
 
 #include <cuda.h>
@@ -27,20 +28,7 @@
 
 namespace uqlbm {
 
-static thread_local std::string g_last_error;
-
-struct LbmError : std::runtime_error {
-    lbm_status code;
-    LbmError(lbm_status c, const std::string &m) : std::runtime_error(m), code(c) {}
-};
-
-#define CU(call)                                                                                          \
-    do {                                                                                                  \
-        cudaError_t e_ = (call);                                                                          \
-        if (e_ != cudaSuccess)                                                                            \
-            throw LbmError(e_ == cudaErrorMemoryAllocation ? LBM_ERR_NOMEM : LBM_ERR_CUDA,                \
-                           std::string(#call) + ": " + cudaGetErrorString(e_));                           \
-    } while (0)
+thread_local std::string g_last_error;
 
 template <class T>
 struct DevBuf {
@@ -99,20 +87,15 @@ static int host_bc_index(const HostSample &s, int i, int pm, int axis, int &mir)
     return i;
 }
 
-// refineInput (cpuLBM.cpp:283-358) + setupVars (cpuLBM.cpp:360-450)
-static HostSample derive(const lbm_config &c, const lbm_init &in)
+// refineInput (cpuLBM.cpp:283-358) + setupVars (cpuLBM.cpp:360-450) for the
+// scalar run parameters.  min_spacing > 0 replaces min(dx, dy) in the CFL
+// time step (non-uniform cells, as LBM.py:215-216 does).
+void derive_scalars(const lbm_config &c, int Nx, int Ny, double min_spacing, ScalarParams &s)
 {
-    HostSample s;
-    if (in.Nx < 3 || in.Ny < 3) throw LbmError(LBM_ERR_INVALID, "Nx and Ny must be at least 3");
+    if (Nx < 3 || Ny < 3) throw LbmError(LBM_ERR_INVALID, "Nx and Ny must be at least 3");
     if (c.RKMETHOD < 0 || c.RKMETHOD > 3) throw LbmError(LBM_ERR_INVALID, "RKMETHOD must be 0..3");
     if (c.FMETHOD < 0 || c.FMETHOD > 1) throw LbmError(LBM_ERR_INVALID, "FMETHOD must be 0 (NND) or 1 (WENO5)");
-    if (!in.bndArray || !in.cellType || !in.density || !in.pressure || !in.temp || !in.velocityX || !in.velocityY ||
-        in.numProps < 1)
-        throw LbmError(LBM_ERR_INVALID, "lbm_init tables missing");
     if (!(c.gamma > 1.0) || !(c.R > 0.0)) throw LbmError(LBM_ERR_INVALID, "gamma must exceed 1 and R be positive");
-    const int Nx = in.Nx, Ny = in.Ny;
-    s.nx = Nx;
-    s.ny = Ny;
     s.rk = c.RKMETHOD;
     s.fm = c.FMETHOD;
     s.flags = (c.periodicX > 0 ? SF_PERX : 0) | (c.periodicY > 0 ? SF_PERY : 0) | (c.mirrorNorth > 0 ? SF_MIRN : 0) |
@@ -126,23 +109,12 @@ static HostSample derive(const lbm_config &c, const lbm_init &in)
     if (dy == 0 && Ly != 0) dy = Ly / ((double)Ny - 1);
     else if (dy == 0 && Ly == 0) { dy = dx; Ly = dy * (Ny - 1); }
     else Ly = dy * (Ny - 1);
+    s.dx = dx;
+    s.dy = dy;
     double rho_ref = c.rho_ref, p_ref = c.p_ref, T_ref = c.T_ref;
     if (rho_ref == 0) rho_ref = p_ref / (c.R * T_ref);
     else if (p_ref == 0) p_ref = rho_ref * c.R * T_ref;
     else if (T_ref == 0) T_ref = p_ref / (rho_ref * c.R);
-    s.dx.resize(Nx);
-    s.dy.resize(Ny);
-    const bool nonuni = c.dx_array || c.dy_array;
-    double mind = std::min(dx, dy);
-    if (nonuni) mind = INFINITY;
-    for (int x = 0; x < Nx; ++x) {
-        s.dx[x] = c.dx_array ? c.dx_array[x] : dx;
-        if (nonuni) mind = std::min(mind, s.dx[x]);
-    }
-    for (int y = 0; y < Ny; ++y) {
-        s.dy[y] = c.dy_array ? c.dy_array[y] : dy;
-        if (nonuni) mind = std::min(mind, s.dy[y]);
-    }
     s.rho_ref = rho_ref;
     s.T_ref = T_ref;
     s.b = 2 / (c.gamma - 1);
@@ -152,15 +124,68 @@ static HostSample derive(const lbm_config &c, const lbm_init &in)
     const double u_ref = std::sqrt(c.R * T_ref);
     const double t_ref = std::max(Lx, Ly) / u_ref;
     s.c = std::sqrt(c.R * s.Tc);
+    const double mind = min_spacing > 0 ? min_spacing : std::min(dx, dy);
     s.dt = c.dtau == 0 ? (c.CFL * mind) / (2 * s.c) : c.dtau * tau_ref;
     if (!(s.dt > 0) || !std::isfinite(s.dt)) throw LbmError(LBM_ERR_INVALID, "derived dt is not positive");
     double ttotal = 0;
     int need = 0;
+    s.nsteps = 0;
     if (c.tt_tref > 0) { ttotal = c.tt_tref * t_ref; need = 1; }
     else if (c.tt_time > 0) { ttotal = c.tt_time; need = 1; }
     else if (c.steps > 0) s.nsteps = c.steps;
     else if (c.tol > 0) s.nsteps = 0;
     if (need) s.nsteps = (int)std::ceil(ttotal / s.dt);
+}
+
+static HostSample derive(const lbm_config &c, const lbm_init &in)
+{
+    HostSample s;
+    if (!in.bndArray || !in.cellType || !in.density || !in.pressure || !in.temp || !in.velocityX || !in.velocityY ||
+        in.numProps < 1)
+        throw LbmError(LBM_ERR_INVALID, "lbm_init tables missing");
+    const int Nx = in.Nx, Ny = in.Ny;
+    if (Nx < 3 || Ny < 3) throw LbmError(LBM_ERR_INVALID, "Nx and Ny must be at least 3");
+    s.nx = Nx;
+    s.ny = Ny;
+    // cell widths first: the CFL step uses their minimum
+    ScalarParams sc;
+    {
+        lbm_config c0 = c;
+        c0.dx_array = nullptr;
+        c0.dy_array = nullptr;
+        ScalarParams tmp;
+        derive_scalars(c0, Nx, Ny, 0.0, tmp);  // completes dx, dy
+        s.dx.assign(Nx, tmp.dx);
+        s.dy.assign(Ny, tmp.dy);
+        double mind = 0.0;
+        if (c.dx_array || c.dy_array) {
+            mind = INFINITY;
+            for (int x = 0; x < Nx; ++x) {
+                if (c.dx_array) s.dx[x] = c.dx_array[x];
+                mind = std::min(mind, s.dx[x]);
+            }
+            for (int y = 0; y < Ny; ++y) {
+                if (c.dy_array) s.dy[y] = c.dy_array[y];
+                mind = std::min(mind, s.dy[y]);
+            }
+        }
+        derive_scalars(c, Nx, Ny, mind, sc);
+    }
+    s.rk = sc.rk;
+    s.fm = sc.fm;
+    s.flags = sc.flags;
+    s.R = sc.R;
+    s.mu = sc.mu;
+    s.Pr = sc.Pr;
+    s.tol = sc.tol;
+    s.rho_ref = sc.rho_ref;
+    s.T_ref = sc.T_ref;
+    s.b = sc.b;
+    s.K = sc.K;
+    s.Tc = sc.Tc;
+    s.c = sc.c;
+    s.dt = sc.dt;
+    s.nsteps = sc.nsteps;
 
     // property tables completed as refineInput does; per-node initial state
     const int np = in.numProps;

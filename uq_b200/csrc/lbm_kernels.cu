@@ -151,14 +151,6 @@ __global__ void __launch_bounds__(256, 2) k_stage0(KArgs<S> a)
 }
 
 // -------------------------------------------------------------------- W
-// wallFluxes (cpuLBM.cpp:1502-1590): for a solid node next to fluid,
-// alpha = (f flux of the fluid 4-neighbours into it) / (|e| f out of it),
-// weighted by the solid cell's 1/dx, 1/dy.
-__constant__ int c_WXX[4] = {-1, 1, 0, 0};
-__constant__ int c_WYY[4] = {0, 0, -1, 1};
-__constant__ int c_WII[4][4] = {{1, 5, 8, 9}, {3, 6, 7, 11}, {2, 5, 6, 10}, {4, 7, 8, 12}};
-__constant__ int c_WINV[4][4] = {{3, 6, 7, 11}, {1, 5, 8, 9}, {4, 8, 7, 12}, {2, 6, 5, 10}};
-
 template <class S, class C>
 __global__ void k_wall(KArgs<S> a, const S *__restrict__ stage, const WallNode *__restrict__ walls, int nwalls)
 {
@@ -167,27 +159,9 @@ __global__ void k_wall(KArgs<S> a, const S *__restrict__ stage, const WallNode *
     const WallNode w = walls[k];
     const SampleParams sp = a.samples[w.sample];
     const StageView<S> v{stage + sp.state_off, a.nflags + sp.node_off, (int)sp.plane, sp.pitch};
-    const double dxm = a.dxv[sp.xoff + w.x], dym = a.dyv[sp.yoff + w.y];
-    const double *fr = a.fref + NPL * w.sample;  // stored values + fr = full values
-    double fin = 0, fout = 0;
-    for (int j = 0; j < 4; ++j) {
-        int m;
-        const int xm = bc_index(sp, w.x, c_WXX[j], 0, m);
-        const int ym = bc_index(sp, w.y, c_WYY[j], 1, m);
-        const uint8_t fl = v.nf[(long long)ym * sp.pitch + xm];
-        if ((fl & NF_TYPE) >= 2) continue;
-        const int axis = j < 2 ? 0 : 1;
-        const double dd = axis == 0 ? dxm : dym;
-        for (int q = 0; q < 4; ++q) {
-            const int i = c_WII[j][q], io = c_WINV[j][q];
-            const double ai = sp.c * abs(axis == 0 ? c_EX[i] : c_EY[i]);
-            const double F = (double)flux_axis<S, C>(sp, v, xm, ym, i, axis, fl) + ai * fr[i];
-            fin += F / dd;
-            const double fo = (double)ldv(v, io, w.x, w.y) + fr[io];
-            fout += fo * (sp.c * abs(axis == 0 ? c_EX[io] : c_EY[io])) / dd;
-        }
-    }
-    a.template alpha_as<C>()[sp.node_off + (long long)w.y * sp.pitch + w.x] = (C)(fin / fout - 1.0);
+    const double am1 = wall_alpha_m1<S, C>(sp, v, w.x, w.y, a.dxv[sp.xoff + w.x], a.dyv[sp.yoff + w.y],
+                                           a.fref + NPL * w.sample);
+    a.template alpha_as<C>()[sp.node_off + (long long)w.y * sp.pitch + w.x] = (C)am1;
 }
 
 // ------------------------------------------------------------------ P1/P2

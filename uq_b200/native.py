@@ -88,6 +88,8 @@ SIGNATURES = {
     "lbm_batch_nodes": (C.c_longlong, [C.c_void_p]),
     "lbm_batch_stream": (C.c_void_p, [C.c_void_p]),
     "lbm_batch_destroy": (None, [C.c_void_p]),
+    "lbm_step_noalloc": (C.c_int, [C.POINTER(LbmConfig), C.c_int, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_int,
+                                   C.c_void_p]),
 }
 
 _lib = None
