@@ -48,8 +48,15 @@ struct SampleParams {
 struct Tile {
     int sample;
     int x0, y0;
-    int gid;  // index of the tile in the batch's full tile list
+    int gid;  // index of the tile in the batch's full tile list; bit 30: simple
 };
+
+// A simple tile lies at least 3 nodes inside its domain and neither it nor
+// its 3-node halo holds a solid/permanent node or a node whose stencil meets
+// a solid or an edge: every flux it needs comes straight from the staged box.
+constexpr int TILE_SIMPLE = 1 << 30;
+__host__ __device__ inline int tile_gid(const Tile &t) { return t.gid & (TILE_SIMPLE - 1); }
+__host__ __device__ inline bool tile_simple(const Tile &t) { return (t.gid & TILE_SIMPLE) != 0; }
 
 // lattice (setupVars, cpuLBM.cpp:376-388) in units of c, its signs, and the
 // reflection maps of mirIndex (cpuLBM.cpp:1147-1169)

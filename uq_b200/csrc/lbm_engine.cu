@@ -410,7 +410,15 @@ struct lbm_batch {
             p.first_tile = (int)tiles_all.size();
             for (int y0 = 0; y0 < h.ny; y0 += ty)
                 for (int x0 = 0; x0 < h.nx; x0 += tx) {
-                    Tile t{k, x0, y0, (int)tiles_all.size()};
+                    int gid = (int)tiles_all.size();
+                    if (x0 >= 3 && y0 >= 3 && x0 + tx + 3 <= h.nx && y0 + ty + 3 <= h.ny) {
+                        bool simple = true;
+                        for (int y = y0 - 3; y < y0 + ty + 3 && simple; ++y)
+                            for (int x = x0 - 3; x < x0 + tx + 3; ++x)
+                                if (flags[p.node_off + (long long)y * p.pitch + x] != 0) { simple = false; break; }
+                        if (simple) gid |= TILE_SIMPLE;
+                    }
+                    Tile t{k, x0, y0, gid};
                     tiles_all.push_back(t);
                     tiles_by_rk[h.rk].push_back(t);
                     if (h.rk == 1) tiles_rk3.push_back(t);

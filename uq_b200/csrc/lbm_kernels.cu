@@ -282,7 +282,7 @@ __device__ __forceinline__ C any_node_flux(TileCtx<S, C> &k, const S *box, int i
 // the tile edges, then the divergence D = (dt/dx, dt/dy).(F_out - F_in) of
 // cFLUX (cpuLBM.cpp:1436-1470).  One copy of the code serves all twelve
 // directions (a compact loop keeps the instruction cache warm).
-template <class S, class C>
+template <class S, class C, bool SIMPLE>
 __device__ __forceinline__ void dir_step(TileCtx<S, C> &k, const int i)
 {
     const int EX = c_EX[i], EY = c_EY[i];
@@ -302,10 +302,34 @@ __device__ __forceinline__ void dir_step(TileCtx<S, C> &k, const int i)
         atomicOr(k.status, STATUS_TIMEOUT);
     }
     const SampleParams &sp = *k.sp;
-    if (k.active) {
+    const C c = (C)sp.c;
+    const C aex = C(abs(EX)) * c, aey = C(abs(EY)) * c;
+    if (SIMPLE) {
+        // every node fluid and fast-path, every upwind neighbour in the box
+        const int lx = k.tx + HALO_X, ly = k.ty + HALO_Y;
+        const S *cf = box + ly * k.BW + lx;
+        const S *ch = cf + k.pstride;
+        if (SX) {
+            sf[k.tid] = box_flux<S, C>(sp, cf, SX, aex);
+            sf[NT + k.tid] = box_flux<S, C>(sp, ch, SX, aex);
+        }
+        if (SY) {
+            sf[2 * NT + k.tid] = box_flux<S, C>(sp, cf, SY * k.BW, aey);
+            sf[3 * NT + k.tid] = box_flux<S, C>(sp, ch, SY * k.BW, aey);
+        }
+        const int nx_items = SX ? 2 * k.TY : 0, ny_items = SY ? 2 * k.TX : 0;
+        const int r = k.tid;
+        if (r < nx_items) {
+            const int fh = r / k.TY, row = r % k.TY;
+            const int bx = (SX > 0 ? -1 : k.TX) + HALO_X, by = row + HALO_Y;
+            ringx[fh * k.TY + row] = box_flux<S, C>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SX, aex);
+        } else if (r < nx_items + ny_items) {
+            const int q = r - nx_items, fh = q / k.TX, col = q % k.TX;
+            const int bx = col + HALO_X, by = (SY > 0 ? -1 : k.TY) + HALO_Y;
+            ringy[fh * k.TX + col] = box_flux<S, C>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SY * k.BW, aey);
+        }
+    } else if (k.active) {
         const int type = k.flag & NF_TYPE;
-        const C c = (C)sp.c;
-        const C aex = C(abs(EX)) * c, aey = C(abs(EY)) * c;
         const int lx = k.tx + HALO_X, ly = k.ty + HALO_Y;
         const S *cf = box + ly * k.BW + lx;
         const S *ch = cf + k.pstride;
@@ -344,7 +368,7 @@ __device__ __forceinline__ void dir_step(TileCtx<S, C> &k, const int i)
         }
     }
     // upwind neighbours outside the tile: index(x, -e) with reflection
-    {
+    if (!SIMPLE) {
         const int nx_items = SX ? 2 * k.TY : 0, ny_items = SY ? 2 * k.TX : 0;
         const int r = k.tid;
         if (r < nx_items) {
@@ -374,7 +398,7 @@ __device__ __forceinline__ void dir_step(TileCtx<S, C> &k, const int i)
     __syncthreads();
     // every thread is done with this slot: refill it three directions ahead
     if (i + NSTAGE <= 12 && k.tid == 0) issue_dir_load(k, i + NSTAGE, slot);
-    if (k.active && (k.flag & NF_TYPE) == 0) {
+    if (SIMPLE || (k.active && (k.flag & NF_TYPE) == 0)) {
         C of = C(0), oh = C(0), inf_ = C(0), inh = C(0);
         bool have = false;
         if (SX) {
@@ -480,8 +504,13 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     const int type = k.flag & NF_TYPE;
     sD[tid] = C(0);          // direction 0 streams nothing
     sD[NQ * NT + tid] = C(0);
+    if (tile_simple(t)) {
 #pragma unroll 1
-    for (int i = 1; i <= 12; ++i) dir_step<S, C>(k, i);
+        for (int i = 1; i <= 12; ++i) dir_step<S, C, true>(k, i);
+    } else {
+#pragma unroll 1
+        for (int i = 1; i <= 12; ++i) dir_step<S, C, false>(k, i);
+    }
 
     double res_part = 0;
     if (active && type == 0) {
@@ -642,7 +671,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
         if (tid == 0) {
             double s = 0;
             for (int w = 0; w < (NT + 31) / 32; ++w) s += red[w];
-            a.partial[t.gid] = s;
+            a.partial[tile_gid(t)] = s;
         }
     }
 }
