@@ -178,28 +178,46 @@ __device__ __forceinline__ C line_flux(const SampleParams &sp, const S *__restri
 
 // Stage tiles in shared memory: per direction the f and h planes over the
 // box [x0-4, x0+TX+4) x [y0-3, y0+TY+3) (x start kept on a 16-byte
-// boundary), loaded by TMA three directions ahead of use.
-constexpr int HALO_X = 4, HALO_Y = 3, NSTAGE = 3;
+// boundary), loaded by TMA ahead of use.  Directions are processed in
+// groups of G (G = 2 pairs each direction with its opposite, halving the
+// barriers; G = 1 on the FP64 path, whose boxes are twice as large).
+constexpr int HALO_X = 4, HALO_Y = 3;
 constexpr uint32_t TMA_WAIT_POLLS = 1u << 16;
+
+template <int G>
+struct GroupCfg {
+    static constexpr int NSTAGE = G == 2 ? 2 : 3;  // groups in flight
+    static constexpr int NGROUP = 12 / G;
+};
+
+// direction m of group g: G = 1 -> 1..12; G = 2 -> (1,3) (2,4) (5,7) (6,8)
+// (9,11) (10,12)
+template <int G>
+__host__ __device__ __forceinline__ int group_dir(int g, int m)
+{
+    if (G == 1) return g + 1;
+    const int base = g < 2 ? g + 1 : (g < 4 ? g + 3 : g + 5);
+    return base + 2 * m;
+}
 
 // Shared-memory layout of k_flux (bytes from a 128-byte aligned base).
 struct FluxSmemLayout {
-    size_t c_elems;      // C arrays: sf[8NT], ring x[4TY], ring y[4TX], sD[26NT]
+    size_t c_elems;      // C arrays: sf[2][G][4][NT], ring x[2][G][2][TY], ring y[2][G][2][TX], sD[26][NT]
     size_t stage_off;    // staged boxes
     size_t plane_bytes;  // one staged plane, padded to 128 bytes
     size_t bar_off;      // NSTAGE mbarriers
     size_t total;        // including 128 bytes of base-alignment slack
 };
 
-__host__ __device__ inline FluxSmemLayout flux_layout(size_t es_c, size_t es_s, int tx, int ty)
+__host__ __device__ inline FluxSmemLayout flux_layout(size_t es_c, size_t es_s, int tx, int ty, int G, int nstage)
 {
     FluxSmemLayout L;
     const size_t NT = (size_t)tx * ty;
-    L.c_elems = 8 * NT + 4 * (size_t)tx + 4 * (size_t)ty + (size_t)NPL * NT;
+    L.c_elems = 8 * (size_t)G * NT + 4 * (size_t)G * tx + 4 * (size_t)G * ty + (size_t)NPL * NT;
     L.stage_off = (L.c_elems * es_c + 127) / 128 * 128;
     L.plane_bytes = ((size_t)(tx + 2 * HALO_X) * (ty + 2 * HALO_Y) * es_s + 127) / 128 * 128;
-    L.bar_off = L.stage_off + (size_t)NSTAGE * 2 * L.plane_bytes;
-    L.total = L.bar_off + NSTAGE * sizeof(uint64_t) + 128;
+    L.bar_off = L.stage_off + (size_t)nstage * 2 * G * L.plane_bytes;
+    L.total = L.bar_off + nstage * sizeof(uint64_t) + 128;
     return L;
 }
 
@@ -209,11 +227,11 @@ struct TileCtx {
     StageView<S> v;
     const C *alpha;  // alpha - 1 of this sample (node-indexed)
     const double *fref;  // this sample's 26 rest-state values
-    C *sf;           // [2 buffers][4: fx_f, fx_h, fy_f, fy_h][NT]
-    C *ringx;        // [2 buffers][2: f, h][TY]
-    C *ringy;        // [2 buffers][2: f, h][TX]
+    C *sf;           // [2 buffers][G][4: fx_f, fx_h, fy_f, fy_h][NT]
+    C *ringx;        // [2 buffers][G][2: f, h][TY]
+    C *ringy;        // [2 buffers][G][2: f, h][TX]
     C *sD;           // [26][NT]
-    const S *stg;    // [NSTAGE][2: f, h][BH][BW], planes `pstride` elements apart
+    const S *stg;    // [NSTAGE][G][2: f, h][BH][BW], planes `pstride` elements apart
     int pstride;
     uint64_t *bars;  // [NSTAGE]
     const CUtensorMap *map;
@@ -225,15 +243,19 @@ struct TileCtx {
     C tdx, tdy;
 };
 
-template <class S, class C>
-__device__ __forceinline__ void issue_dir_load(TileCtx<S, C> &k, int dir, int slot)
+template <int G, class S, class C>
+__device__ __forceinline__ void issue_group_load(TileCtx<S, C> &k, int g, int slot)
 {
     const uint32_t box = (uint32_t)(k.BW * k.BH * sizeof(S));
-    S *dst = const_cast<S *>(k.stg) + (size_t)slot * 2 * k.pstride;
+    S *dst = const_cast<S *>(k.stg) + (size_t)slot * 2 * G * k.pstride;
     fence_proxy_async_smem();
-    mbar_arrive_expect_tx(&k.bars[slot], 2 * box);
-    tma_load_3d(dst, k.map, k.x0 - HALO_X, k.y0 - HALO_Y, dir, &k.bars[slot]);
-    tma_load_3d(dst + k.pstride, k.map, k.x0 - HALO_X, k.y0 - HALO_Y, NQ + dir, &k.bars[slot]);
+    mbar_arrive_expect_tx(&k.bars[slot], 2 * G * box);
+#pragma unroll
+    for (int m = 0; m < G; ++m) {
+        const int dir = group_dir<G>(g, m);
+        tma_load_3d(dst + (size_t)(2 * m) * k.pstride, k.map, k.x0 - HALO_X, k.y0 - HALO_Y, dir, &k.bars[slot]);
+        tma_load_3d(dst + (size_t)(2 * m + 1) * k.pstride, k.map, k.x0 - HALO_X, k.y0 - HALO_Y, NQ + dir, &k.bars[slot]);
+    }
 }
 
 // reconstruction from the staged box (fast path; no solid, no domain edge
@@ -276,34 +298,21 @@ __device__ __forceinline__ C any_node_flux(TileCtx<S, C> &k, const S *box, int i
     return flux_axis<S, C>(sp, k.v, xn, yn, pp, axis, fl);
 }
 
-// Direction i (1..12): outgoing face fluxes of the f and h planes at this
-// node (posFluxes/computeFlux, cpuLBM.cpp:1405-1500; a solid node answers
-// wallFluxes' alpha |e| f, cpuLBM.cpp:1576-1586), the upwind fluxes across
-// the tile edges, then the divergence D = (dt/dx, dt/dy).(F_out - F_in) of
-// cFLUX (cpuLBM.cpp:1436-1470).  One copy of the code serves all twelve
-// directions (a compact loop keeps the instruction cache warm).
+// Own-node face fluxes of direction i into sf_m (fx_f, fx_h, fy_f, fy_h)
+// and the upwind fluxes across the tile edges into ringx_m / ringy_m
+// (items numbered from ring0 over the block's threads).
 template <class S, class C, bool SIMPLE>
-__device__ __forceinline__ void dir_step(TileCtx<S, C> &k, const int i)
+__device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const S *box, C *sf, C *ringx, C *ringy,
+                                           int ring0)
 {
     const int EX = c_EX[i], EY = c_EY[i];
     const int SX = isgn(EX), SY = isgn(EY);
-    const int buf = i & 1;
-    const int slot = (i - 1) % NSTAGE;
-    const uint32_t parity = ((i - 1) / NSTAGE) & 1;
     const int NT = k.NT;
-    C *sf = k.sf + buf * 4 * NT;
-    C *ringx = k.ringx + buf * 2 * k.TY;
-    C *ringy = k.ringy + buf * 2 * k.TX;
-    const S *box = k.stg + (size_t)slot * 2 * k.pstride;
-    // every issued copy is waited for (boundedly), also after a timeout, so
-    // no copy is still in flight when the block exits
-    if (!mbar_wait_bounded(&k.bars[slot], parity, TMA_WAIT_POLLS)) {
-        *k.timed_out = 1;
-        atomicOr(k.status, STATUS_TIMEOUT);
-    }
     const SampleParams &sp = *k.sp;
     const C c = (C)sp.c;
     const C aex = C(abs(EX)) * c, aey = C(abs(EY)) * c;
+    const int nx_items = SX ? 2 * k.TY : 0, ny_items = SY ? 2 * k.TX : 0;
+    const int r = k.tid - ring0;
     if (SIMPLE) {
         // every node fluid and fast-path, every upwind neighbour in the box
         const int lx = k.tx + HALO_X, ly = k.ty + HALO_Y;
@@ -317,18 +326,18 @@ __device__ __forceinline__ void dir_step(TileCtx<S, C> &k, const int i)
             sf[2 * NT + k.tid] = box_flux<S, C>(sp, cf, SY * k.BW, aey);
             sf[3 * NT + k.tid] = box_flux<S, C>(sp, ch, SY * k.BW, aey);
         }
-        const int nx_items = SX ? 2 * k.TY : 0, ny_items = SY ? 2 * k.TX : 0;
-        const int r = k.tid;
-        if (r < nx_items) {
+        if (r >= 0 && r < nx_items) {
             const int fh = r / k.TY, row = r % k.TY;
             const int bx = (SX > 0 ? -1 : k.TX) + HALO_X, by = row + HALO_Y;
             ringx[fh * k.TY + row] = box_flux<S, C>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SX, aex);
-        } else if (r < nx_items + ny_items) {
+        } else if (r >= nx_items && r < nx_items + ny_items) {
             const int q = r - nx_items, fh = q / k.TX, col = q % k.TX;
             const int bx = col + HALO_X, by = (SY > 0 ? -1 : k.TY) + HALO_Y;
             ringy[fh * k.TX + col] = box_flux<S, C>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SY * k.BW, aey);
         }
-    } else if (k.active) {
+        return;
+    }
+    if (k.active) {
         const int type = k.flag & NF_TYPE;
         const int lx = k.tx + HALO_X, ly = k.ty + HALO_Y;
         const S *cf = box + ly * k.BW + lx;
@@ -368,76 +377,128 @@ __device__ __forceinline__ void dir_step(TileCtx<S, C> &k, const int i)
         }
     }
     // upwind neighbours outside the tile: index(x, -e) with reflection
-    if (!SIMPLE) {
-        const int nx_items = SX ? 2 * k.TY : 0, ny_items = SY ? 2 * k.TX : 0;
-        const int r = k.tid;
-        if (r < nx_items) {
-            const int fh = r / k.TY, row = r % k.TY, yy = k.y0 + row;
-            C val = C(0);
-            if (yy < k.y_end) {
-                int m;
-                const int xn = SX > 0 ? k.x0 : k.x_end - 1;
-                const int xr = bc_index(sp, xn, -SX, 0, m);
-                const bool in_box = !m && xr == xn - SX;
-                val = any_node_flux<S, C>(k, box, i, xr, yy, fh, 0, m != 0, in_box);
-            }
-            ringx[fh * k.TY + row] = val;
-        } else if (r < nx_items + ny_items) {
-            const int q = r - nx_items, fh = q / k.TX, col = q % k.TX, xx = k.x0 + col;
-            C val = C(0);
-            if (xx < k.x_end) {
-                int m;
-                const int yn = SY > 0 ? k.y0 : k.y_end - 1;
-                const int yr = bc_index(sp, yn, -SY, 1, m);
-                const bool in_box = !m && yr == yn - SY;
-                val = any_node_flux<S, C>(k, box, i, xx, yr, fh, 1, m != 0, in_box);
-            }
-            ringy[fh * k.TX + col] = val;
+    if (r >= 0 && r < nx_items) {
+        const int fh = r / k.TY, row = r % k.TY, yy = k.y0 + row;
+        C val = C(0);
+        if (yy < k.y_end) {
+            int m;
+            const int xn = SX > 0 ? k.x0 : k.x_end - 1;
+            const int xr = bc_index(sp, xn, -SX, 0, m);
+            const bool in_box = !m && xr == xn - SX;
+            val = any_node_flux<S, C>(k, box, i, xr, yy, fh, 0, m != 0, in_box);
         }
+        ringx[fh * k.TY + row] = val;
+    } else if (r >= nx_items && r < nx_items + ny_items) {
+        const int q = r - nx_items, fh = q / k.TX, col = q % k.TX, xx = k.x0 + col;
+        C val = C(0);
+        if (xx < k.x_end) {
+            int m;
+            const int yn = SY > 0 ? k.y0 : k.y_end - 1;
+            const int yr = bc_index(sp, yn, -SY, 1, m);
+            const bool in_box = !m && yr == yn - SY;
+            val = any_node_flux<S, C>(k, box, i, xx, yr, fh, 1, m != 0, in_box);
+        }
+        ringy[fh * k.TX + col] = val;
     }
-    __syncthreads();
-    // every thread is done with this slot: refill it three directions ahead
-    if (i + NSTAGE <= 12 && k.tid == 0) issue_dir_load(k, i + NSTAGE, slot);
-    if (SIMPLE || (k.active && (k.flag & NF_TYPE) == 0)) {
-        C of = C(0), oh = C(0), inf_ = C(0), inh = C(0);
-        bool have = false;
-        if (SX) {
-            const int xu = k.x - SX;
-            const bool inside = xu >= k.x0 && xu < k.x_end;
-            const C fi = inside ? sf[k.tid - SX] : ringx[k.ty];
-            const C hi = inside ? sf[NT + k.tid - SX] : ringx[k.TY + k.ty];
-            of = k.tdx * sf[k.tid];
-            oh = k.tdx * sf[NT + k.tid];
-            inf_ = k.tdx * fi;
-            inh = k.tdx * hi;
-            have = true;
-        }
-        if (SY) {
-            const int yu = k.y - SY;
-            const bool inside = yu >= k.y0 && yu < k.y_end;
-            const C fi = inside ? sf[2 * NT + k.tid - SY * k.TX] : ringy[k.tx];
-            const C hi = inside ? sf[3 * NT + k.tid - SY * k.TX] : ringy[k.TX + k.tx];
-            if (have) {
-                of = of + k.tdy * sf[2 * NT + k.tid];
-                oh = oh + k.tdy * sf[3 * NT + k.tid];
-                inf_ = inf_ + k.tdy * fi;
-                inh = inh + k.tdy * hi;
-            } else {
-                of = k.tdy * sf[2 * NT + k.tid];
-                oh = k.tdy * sf[3 * NT + k.tid];
-                inf_ = k.tdy * fi;
-                inh = k.tdy * hi;
-            }
-        }
-        k.sD[i * NT + k.tid] = of - inf_;
-        k.sD[(NQ + i) * NT + k.tid] = oh - inh;
-    }
-    // sf and the rings are double-buffered by direction parity: buffer
-    // (i & 1) is written again at direction i + 2, after direction i + 1's
-    // barrier, which every reader of this direction has passed.
 }
 
-size_t flux_smem_bytes_t(size_t es, int tx, int ty) { return flux_layout(es, es, tx, ty).total; }
+// divergence D = (dt/dx, dt/dy).(F_out - F_in) of cFLUX
+// (cpuLBM.cpp:1436-1470) for direction i at this node
+template <class S, class C>
+__device__ __forceinline__ void dir_divergence(TileCtx<S, C> &k, const int i, const C *sf, const C *ringx,
+                                               const C *ringy)
+{
+    const int SX = isgn(c_EX[i]), SY = isgn(c_EY[i]);
+    const int NT = k.NT;
+    C of = C(0), oh = C(0), inf_ = C(0), inh = C(0);
+    bool have = false;
+    if (SX) {
+        const int xu = k.x - SX;
+        const bool inside = xu >= k.x0 && xu < k.x_end;
+        const C fi = inside ? sf[k.tid - SX] : ringx[k.ty];
+        const C hi = inside ? sf[NT + k.tid - SX] : ringx[k.TY + k.ty];
+        of = k.tdx * sf[k.tid];
+        oh = k.tdx * sf[NT + k.tid];
+        inf_ = k.tdx * fi;
+        inh = k.tdx * hi;
+        have = true;
+    }
+    if (SY) {
+        const int yu = k.y - SY;
+        const bool inside = yu >= k.y0 && yu < k.y_end;
+        const C fi = inside ? sf[2 * NT + k.tid - SY * k.TX] : ringy[k.tx];
+        const C hi = inside ? sf[3 * NT + k.tid - SY * k.TX] : ringy[k.TX + k.tx];
+        if (have) {
+            of = of + k.tdy * sf[2 * NT + k.tid];
+            oh = oh + k.tdy * sf[3 * NT + k.tid];
+            inf_ = inf_ + k.tdy * fi;
+            inh = inh + k.tdy * hi;
+        } else {
+            of = k.tdy * sf[2 * NT + k.tid];
+            oh = k.tdy * sf[3 * NT + k.tid];
+            inf_ = k.tdy * fi;
+            inh = k.tdy * hi;
+        }
+    }
+    k.sD[i * NT + k.tid] = of - inf_;
+    k.sD[(NQ + i) * NT + k.tid] = oh - inh;
+}
+
+// Group g of G directions: wait for its staged boxes, the face fluxes
+// (posFluxes/computeFlux, cpuLBM.cpp:1405-1500; solid nodes answer
+// wallFluxes' alpha |e| f, cpuLBM.cpp:1576-1586) and edge fluxes of each,
+// one barrier, refill the slot, then each direction's divergence.
+template <class S, class C, bool SIMPLE, int G>
+__device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
+{
+    constexpr int NST = GroupCfg<G>::NSTAGE;
+    const int buf = g & 1;
+    const int slot = g % NST;
+    const uint32_t parity = (g / NST) & 1;
+    const int NT = k.NT;
+    // every issued copy is waited for (boundedly), also after a timeout, so
+    // no copy is still in flight when the block exits
+    if (!mbar_wait_bounded(&k.bars[slot], parity, TMA_WAIT_POLLS)) {
+        *k.timed_out = 1;
+        atomicOr(k.status, STATUS_TIMEOUT);
+    }
+    const S *boxes = k.stg + (size_t)slot * 2 * G * k.pstride;
+    int ring0 = 0;
+#pragma unroll 1
+    for (int m = 0; m < G; ++m) {
+        const int i = group_dir<G>(g, m);
+        C *sf = k.sf + (size_t)(buf * G + m) * 4 * NT;
+        C *rx = k.ringx + (size_t)(buf * G + m) * 2 * k.TY;
+        C *ry = k.ringy + (size_t)(buf * G + m) * 2 * k.TX;
+        dir_fluxes<S, C, SIMPLE>(k, i, boxes + (size_t)(2 * m) * k.pstride, sf, rx, ry, ring0);
+        ring0 += (c_EX[i] ? 2 * k.TY : 0) + (c_EY[i] ? 2 * k.TX : 0);
+    }
+    __syncthreads();
+    // every thread is done with this slot: refill it NST groups ahead
+    if (g + NST < GroupCfg<G>::NGROUP && k.tid == 0) issue_group_load<G>(k, g + NST, slot);
+    if (SIMPLE || (k.active && (k.flag & NF_TYPE) == 0)) {
+#pragma unroll 1
+        for (int m = 0; m < G; ++m) {
+            const int i = group_dir<G>(g, m);
+            dir_divergence<S, C>(k, i, k.sf + (size_t)(buf * G + m) * 4 * NT,
+                                 k.ringx + (size_t)(buf * G + m) * 2 * k.TY, k.ringy + (size_t)(buf * G + m) * 2 * k.TX);
+        }
+    }
+    // sf and the rings are double-buffered by group parity: buffer (g & 1)
+    // is written again at group g + 2, after group g + 1's barrier, which
+    // every reader of this group has passed.
+}
+
+template <class S>
+struct FluxGroup {
+    static constexpr int value = sizeof(S) == 4 ? 2 : 1;
+};
+
+size_t flux_smem_bytes_t(size_t es, int tx, int ty)
+{
+    const int G = es == 4 ? 2 : 1;
+    return flux_layout(es, es, tx, ty, G, G == 2 ? GroupCfg<2>::NSTAGE : GroupCfg<1>::NSTAGE).total;
+}
 
 // MODE: 1 = RK3 stage 3 (fluxes of buffer 2), 2 = RK3 final (buffer 3),
 // 3 = RK1 update, 4 = EULER update, 5 = EULER_EQ update (buffer 2)
@@ -447,12 +508,14 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     const int TX = a.tx, TY = a.ty, NT = TX * TY;
     const int BW = TX + 2 * HALO_X, BH = TY + 2 * HALO_Y;
-    const FluxSmemLayout Ls = flux_layout(sizeof(C), sizeof(S), TX, TY);
+    constexpr int G = FluxGroup<S>::value;
+    constexpr int NST = GroupCfg<G>::NSTAGE;
+    const FluxSmemLayout Ls = flux_layout(sizeof(C), sizeof(S), TX, TY, G, NST);
     unsigned char *smem_raw = smem_dyn + ((128 - (smem_u32(smem_dyn) & 127)) & 127);
-    C *sf = reinterpret_cast<C *>(smem_raw);  // [2][4][NT]
-    C *ringx = sf + 8 * NT;                    // [2][2][TY]
-    C *ringy = ringx + 4 * TY;                 // [2][2][TX]
-    C *sD = ringy + 4 * TX;                    // [26][NT]
+    C *sf = reinterpret_cast<C *>(smem_raw);  // [2][G][4][NT]
+    C *ringx = sf + 8 * G * NT;                // [2][G][2][TY]
+    C *ringy = ringx + 4 * G * TY;             // [2][G][2][TX]
+    C *sD = ringy + 4 * G * TX;                // [26][NT]
     S *stg = reinterpret_cast<S *>(smem_raw + Ls.stage_off);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + Ls.bar_off);
     __shared__ double red[32];
@@ -471,9 +534,9 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     if (tid == 0) {
         s_sp = a.samples[t.sample];
         s_timeout = 0;
-        for (int b = 0; b < NSTAGE; ++b) mbar_init(&bars[b], 1);
+        for (int b = 0; b < NST; ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
-        for (int d = 1; d <= NSTAGE; ++d) issue_dir_load(k, d, d - 1);
+        for (int g = 0; g < NST; ++g) issue_group_load<G>(k, g, g);
     }
     __syncthreads();
     const SampleParams &sp = s_sp;
@@ -506,10 +569,10 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     sD[NQ * NT + tid] = C(0);
     if (tile_simple(t)) {
 #pragma unroll 1
-        for (int i = 1; i <= 12; ++i) dir_step<S, C, true>(k, i);
+        for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G>(k, g);
     } else {
 #pragma unroll 1
-        for (int i = 1; i <= 12; ++i) dir_step<S, C, false>(k, i);
+        for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, false, G>(k, g);
     }
 
     double res_part = 0;
