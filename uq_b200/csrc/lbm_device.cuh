@@ -43,6 +43,7 @@ struct SampleParams {
     // holds f - f_ref, h - h_ref with f_ref, h_ref the equilibria at
     // (rho0, 0, 0, T0); rho0 = shref = 0 (full storage) on the FP64 path.
     double rho0, T0n, shref;  // T0n = T0 / Tc
+    double inv_mu, two_over_bR;
 };
 
 struct Tile {
@@ -358,10 +359,13 @@ __device__ __forceinline__ void eq_all(const EqState<C> &q, C *f, C *h)
 
 // ---------------------------------------------------------------- moments
 // macroProp/macroPropShort (cpuLBM.cpp:877-970): FP64 sums over the node's
-// 13 f and 13 h values; tau_f = mu/p, tau_h = tau_f/Pr,
-// tau_hf = tau_h tau_f / (tau_f - tau_h) (cpuLBM.cpp:952-955).
+// 13 f and 13 h values.  The relaxation times tau_f = mu/p, tau_h =
+// tau_f/Pr, tau_hf = tau_h tau_f / (tau_f - tau_h) (cpuLBM.cpp:952-955)
+// enter every formula as their inverses, which are all linear in
+// q = p / mu: 1/tau_f = q, 1/tau_h = Pr q, 1/tau_hf = (Pr - 1) q (so
+// Pr = 1 gives 1/tau_hf = 0, the reference's x / inf).
 struct Macro {
-    double rho, ux, uy, T, p, tf, th, thf;
+    double rho, ux, uy, T, p, q;
 };
 
 __device__ __forceinline__ Macro macro_from_sums(double r, double rux, double ruy, double sh, const SampleParams &sp)
@@ -371,15 +375,14 @@ __device__ __forceinline__ Macro macro_from_sums(double r, double rux, double ru
     r = sp.rho0 + r;
     sh = sp.shref + sh;
     Macro m;
+    const double ir = 1.0 / r;
     m.rho = r;
-    m.ux = rux / r;
-    m.uy = ruy / r;
+    m.ux = rux * ir;
+    m.uy = ruy * ir;
     const double usq = m.ux * m.ux + m.uy * m.uy;
-    m.T = 2.0 * (sh / r - usq / 2.0) / sp.bR;
+    m.T = (sh * ir - 0.5 * usq) * sp.two_over_bR;
     m.p = r * sp.R * m.T;
-    m.tf = sp.mu / m.p;
-    m.th = m.tf / sp.Pr;
-    m.thf = (m.th * m.tf) / (m.tf - m.th);
+    m.q = m.p * sp.inv_mu;
     return m;
 }
 

@@ -354,6 +354,8 @@ struct lbm_batch {
             p.Pr = h.Pr;
             p.dt = h.dt;
             p.c = h.c;
+            p.inv_mu = 1.0 / h.mu;
+            p.two_over_bR = 2.0 / (h.b * h.R);
             // rest state of the stored deviations (FP32 path only)
             if (prec == LBM_PREC_F32) {
                 p.rho0 = (h.rho_ref > 0 && std::isfinite(h.rho_ref)) ? h.rho_ref : 1.0;

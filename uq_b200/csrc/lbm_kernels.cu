@@ -118,32 +118,35 @@ __global__ void __launch_bounds__(256, 2) k_stage0(KArgs<S> a)
             atomicOr(&a.status[t.sample], STATUS_EQ);
     }
     const C dt = (C)sp.dt, ux = (C)m.ux, uy = (C)m.uy;
-    const C tf = (C)m.tf, th = (C)m.th, thf = (C)m.thf;
+    const C rq = (C)m.q, Pr = (C)sp.Pr;  // 1/tau_f
     if (RK == 1) {
         // RK3 stages 1 and 2 (cpuLBM.cpp:1819-1924); stage 2 reuses stage 1's
-        // equilibrium, moments and relaxation times.
-        const C cf = dt / (C(2) * tf), ch = dt / (C(2) * th), chf = dt / (C(2) * thf);
+        // equilibrium, moments and relaxation times.  cf = dt/(2 tau_f),
+        // ch = dt/(2 tau_h), g = 1/tau_hf.
+        const C hdt = C(0.5) * dt;
+        const C cf = hdt * rq, ch = hdt * Pr * rq, g = (Pr - C(1)) * rq;
+        const C icf = C(1) / (C(1) + cf), ich = C(1) / (C(1) + ch);
 #pragma unroll
         for (int i = 0; i < NQ; ++i) {
             const C f = (C)st[(long long)i * sp.plane + o], h = (C)st[(long long)(NQ + i) * sp.plane + o];
             const C eu = (C)(sp.c * c_EX[i]) * ux + (C)(sp.c * c_EY[i]) * uy;
-            const C f1 = (f + cf * fe[i]) / (C(1) + cf);
-            const C h1 = (h - chf * eu * (fe[i] - f1) + ch * he[i]) / (C(1) + ch);
-            const C f2 = (f - cf * (fe[i] - f1) + cf * fe[i]) / (C(1) + cf);
-            const C h2 = (h - (dt / C(2)) * ((eu / thf) * (fe[i] - f2) - (eu / thf) * (fe[i] - f1)) - ch * (he[i] - h1) + ch * he[i])
-                         / (C(1) + ch);
+            const C f1 = (f + cf * fe[i]) * icf;
+            const C h1 = (h - hdt * g * eu * (fe[i] - f1) + ch * he[i]) * ich;
+            const C f2 = (f - cf * (fe[i] - f1) + cf * fe[i]) * icf;
+            const C h2 = (h - hdt * (eu * g * (fe[i] - f2) - eu * g * (fe[i] - f1)) - ch * (he[i] - h1) + ch * he[i]) * ich;
             b2[(long long)i * sp.plane + o] = (S)f2;
             b2[(long long)(NQ + i) * sp.plane + o] = (S)h2;
         }
     } else {
         // RK1 stage 1 (cpuLBM.cpp:1619-1663)
-        const C cf = dt / tf, ch = dt / th;
+        const C cf = dt * rq, ch = dt * Pr * rq, g = (Pr - C(1)) * rq;
+        const C icf = C(1) / (C(1) + cf), ich = C(1) / (C(1) + ch);
 #pragma unroll
         for (int i = 0; i < NQ; ++i) {
             const C f = (C)st[(long long)i * sp.plane + o], h = (C)st[(long long)(NQ + i) * sp.plane + o];
             const C eu = (C)(sp.c * c_EX[i]) * ux + (C)(sp.c * c_EY[i]) * uy;
-            const C f1 = (f + cf * fe[i]) / (C(1) + cf);
-            const C h1 = (h - dt * eu * ((fe[i] - f1) / thf) + ch * he[i]) / (C(1) + ch);
+            const C f1 = (f + cf * fe[i]) * icf;
+            const C h1 = (h - dt * eu * ((fe[i] - f1) * g) + ch * he[i]) * ich;
             b2[(long long)i * sp.plane + o] = (S)f1;
             b2[(long long)(NQ + i) * sp.plane + o] = (S)h1;
         }
@@ -590,11 +593,11 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             // (macroProp3, cpuLBM.cpp:973-1032), both summed in FP64
             constexpr bool DEV = sizeof(S) == 4;
             Macro m1, m3;
-            C tf2, th2, thf2, tf3, th3, thf3, ux1, uy1, ux3, uy3;
+            C rq1, rq3, ux1, uy1, ux3, uy3;
             double rho3;
             {
                 m1 = node_macro(st, sp, o);
-                tf2 = (C)m1.tf; th2 = (C)m1.th; thf2 = (C)m1.thf; ux1 = (C)m1.ux; uy1 = (C)m1.uy;
+                rq1 = (C)m1.q; ux1 = (C)m1.ux; uy1 = (C)m1.uy;
             }
             {
                 double r = 0, rux = 0, ruy = 0, sh = 0;
@@ -608,16 +611,18 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     sh += (double)st[(long long)(NQ + i) * sp.plane + o] - (double)sD[(NQ + i) * NT + tid];
                 }
                 m3 = macro_from_sums(r, rux, ruy, sh, sp);
-                tf3 = (C)m3.tf; th3 = (C)m3.th; thf3 = (C)m3.thf; ux3 = (C)m3.ux; uy3 = (C)m3.uy;
+                rq3 = (C)m3.q; ux3 = (C)m3.ux; uy3 = (C)m3.uy;
                 rho3 = m3.rho;
             }
             const EqArgs<C, DEV> q1(m1.rho, m1.ux, m1.uy, m1.T, sp);
             const EqArgs<C, DEV> q3(m3.rho, m3.ux, m3.uy, m3.T, sp);
             const C hdt = dt * C(0.5);
-            const C a2 = hdt / tf2, a3 = hdt / tf3, b2c = hdt / th2, b3c = hdt / th3;
+            // dt/(2 tau) and 1/tau of stages 2 (= 1) and 3, all from q = p/mu
+            const C Pr = (C)sp.Pr;
+            const C itf2 = rq1, itf3 = rq3, ith2 = Pr * rq1, ith3 = Pr * rq3;
+            const C g2 = (Pr - C(1)) * rq1, g3 = (Pr - C(1)) * rq3;
+            const C a2 = hdt * itf2, a3 = hdt * itf3, b2c = hdt * ith2, b3c = hdt * ith3;
             const C ia3 = C(1) / (C(1) + a3), ib3 = C(1) / (C(1) + b3c);
-            const C g2 = C(1) / thf2, g3 = C(1) / thf3, itf2 = C(1) / tf2, itf3 = C(1) / tf3;
-            const C ith2 = C(1) / th2, ith3 = C(1) / th3;
             double sf3 = 0;
 #pragma unroll 1
             for (int fam = 0; fam < 4; ++fam) {
@@ -671,7 +676,8 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             const Macro m = node_macro(st, sp, o);
             constexpr bool DEV = sizeof(S) == 4;
             const EqArgs<C, DEV> q(m.rho, m.ux, m.uy, m.T, sp);
-            const C tf = (C)m.tf, th = (C)m.th, thf = (C)m.thf, ux = (C)m.ux, uy = (C)m.uy;
+            const C ux = (C)m.ux, uy = (C)m.uy, Pr = (C)sp.Pr;
+            const C rtf = dt * (C)m.q, rth = dt * Pr * (C)m.q, rg = (Pr - C(1)) * (C)m.q;  // dt/tau_f, dt/tau_h, 1/tau_hf
             double sf = 0;
 #pragma unroll 1
             for (int fam = 0; fam < 4; ++fam) {
@@ -698,11 +704,11 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     C fn, hn;
                     if (MODE == 3) {
                         const C f1 = v1f[k], h1 = v1h[k];
-                        fn = f - Df + (dt / tf) * (fe[k] - f1);
-                        hn = h - Dh + (dt / th) * (he[k] - h1) - ((dt * eu) / thf) * (fe[k] - f1);
+                        fn = f - Df + rtf * (fe[k] - f1);
+                        hn = h - Dh + rth * (he[k] - h1) - (dt * eu * rg) * (fe[k] - f1);
                     } else if (MODE == 4) {
-                        fn = f - Df + (dt / tf) * (fe[k] - f);
-                        hn = h - Dh + (dt / th) * (he[k] - h) - ((dt * eu) / thf) * (fe[k] - f);
+                        fn = f - Df + rtf * (fe[k] - f);
+                        hn = h - Dh + rth * (he[k] - h) - (dt * eu * rg) * (fe[k] - f);
                     } else {
                         fn = fe[k] - Df;
                         hn = he[k] - Dh;
@@ -715,14 +721,24 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                 atomicOr(&a.status[t.sample], STATUS_EQ);
         }
         if (final_phase) {
-            // macroPropShort of the new state: the residual's T and a
-            // finiteness / positive-density check
-            const Macro mn = node_macro(st, sp, o);
-            if (!(mn.rho > 0.0) || !isfinite(mn.rho) || !isfinite(mn.T) || !isfinite(mn.ux) || !isfinite(mn.uy))
-                atomicOr(&a.status[t.sample], STATUS_NONFINITE);
             if (a.want_residual) {
+                // macroPropShort of the new state: the residual's T, and the
+                // finiteness / positive-density check
+                const Macro mn = node_macro(st, sp, o);
+                if (!(mn.rho > 0.0) || !isfinite(mn.rho) || !isfinite(mn.T) || !isfinite(mn.ux) || !isfinite(mn.uy))
+                    atomicOr(&a.status[t.sample], STATUS_NONFINITE);
                 const double d = mn.T - a.told[sp.node_off + o];
                 res_part = d * d;
+            } else {
+                // finiteness / positive density from the FP64 sums alone
+                double r = 0, sh = 0;
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) {
+                    r += (double)st[(long long)i * sp.plane + o];
+                    sh += (double)st[(long long)(NQ + i) * sp.plane + o];
+                }
+                r += sp.rho0;
+                if (!(r > 0.0) || !isfinite(r) || !isfinite(sh)) atomicOr(&a.status[t.sample], STATUS_NONFINITE);
             }
         }
     }

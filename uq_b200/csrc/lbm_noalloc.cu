@@ -227,6 +227,8 @@ static lbm_status step_noalloc(const lbm_config *cfg, int Nx, int Ny, const int 
     sp.Pr = sc.Pr;
     sp.dt = sc.dt;
     sp.c = sc.c;
+    sp.inv_mu = 1.0 / sc.mu;
+    sp.two_over_bR = 2.0 / (sc.b * sc.R);
     sp.rho0 = 0.0;
     sp.T0n = 1.0;
     sp.shref = 0.0;
