@@ -170,6 +170,13 @@ LBM_API lbm_status lbm_batch_set_macro(lbm_batch *b, int sample, const double *r
  * phase_ms[0..5]: pointwise stages, walls of buffer 2, stencil phase 1,
  * walls of buffer 3, stencil phase 2, residual reduction. */
 LBM_API lbm_status lbm_batch_profile(lbm_batch *b, int n_steps, double *phase_ms, int n_phases);
+/* Autotuner: time n-step runs (CUDA events) of the batch for each
+ * candidate tile shape (pairs tile_x, tile_y; NULL / 0 candidates: a
+ * built-in list), switch the batch to the fastest and restore the state it
+ * had, so tuning leaves results unchanged.  chosen (2 ints) and
+ * ms_per_step (one per candidate) may be NULL. */
+LBM_API lbm_status lbm_batch_autotune(lbm_batch *b, const int *candidates, int n_candidates, int steps, int *chosen,
+                                      double *ms_per_step);
 /* Kernel launches one step of the batch issues. */
 LBM_API int lbm_batch_launches_per_step(lbm_batch *b, int want_residual);
 /* Lattice updates (nodes) one step of the whole batch performs. */

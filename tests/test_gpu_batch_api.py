@@ -28,3 +28,31 @@ def test_profile_and_launch_count(cuda_device):
     assert ms.shape == (6,) and (ms[:5] >= 0).all() and ms[2] > 0
     assert b.launches_per_step(False) == 5
     assert b.launches_per_step(True) == 6
+
+
+def test_tile_shape_does_not_change_results(cuda_device):
+    cases = [W.couette(nx=70, ny=52, steps=4, seed=1), W.random_state(33, 41, seed=2, bc="mirror", solid_frac=0.1,
+                                                                      du=0.02, drho=0.02, dT=0.02, steps=4)]
+    ref = Batch(cases, "f32", tile=(32, 8))
+    ref.step(4)
+    for tile in ((16, 16), (8, 32), (64, 4)):
+        b = Batch(cases, "f32", tile=tile)
+        b.step(4)
+        for k in range(len(cases)):
+            assert np.array_equal(b.dist(k)[0], ref.dist(k)[0]), tile
+
+
+def test_autotune_keeps_state_and_results(cuda_device):
+    cases = [W.couette(nx=96, ny=80, steps=6, seed=3), W.couette(nx=64, ny=64, steps=6, seed=4, u_w=0.15)]
+    a = Batch(cases, "f32")
+    b = Batch(cases, "f32")
+    a.step(2)
+    b.step(2)
+    f_before = b.dist(0)[0]
+    chosen, table = b.autotune([(16, 16), (32, 8)], steps=1)
+    assert chosen in ((16, 16), (32, 8)) and set(table) == {(16, 16), (32, 8)}
+    assert np.array_equal(b.dist(0)[0], f_before)
+    a.step(3)
+    b.step(3)
+    for k in range(2):
+        assert np.array_equal(a.dist(k)[0], b.dist(k)[0])

@@ -243,7 +243,10 @@ using namespace uqlbm;
 
 struct lbm_batch {
     int prec = LBM_PREC_F64;
-    int tx = 32, ty = 8;
+    // default tile: the autotuner's pick on the 512-sample UQ ensemble, both
+    // precisions (lbm_batch_autotune re-measures for a given batch)
+    int tx = 16, ty = 16;
+    std::vector<uint8_t> flags_host;
     bool use_graph = true;
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -278,6 +281,136 @@ struct lbm_batch {
         for (auto &g : graph)
             if (g) cudaGraphExecDestroy(g);
         if (stream) cudaStreamDestroy(stream);
+    }
+
+    // Tile lists for the current tile shape: every sample cut into tx x ty
+    // tiles, each flagged simple when it and its 3-node halo lie inside the
+    // domain and hold only plain fluid nodes.
+    void make_tiles()
+    {
+        tiles_all.clear();
+        tiles_rk3.clear();
+        for (auto &v : tiles_by_rk) v.clear();
+        tile_first.clear();
+        tile_count.clear();
+        for (size_t k = 0; k < hs.size(); ++k) {
+            const HostSample &h = hs[k];
+            SampleParams &p = sp[k];
+            p.first_tile = (int)tiles_all.size();
+            for (int y0 = 0; y0 < h.ny; y0 += ty)
+                for (int x0 = 0; x0 < h.nx; x0 += tx) {
+                    int gid = (int)tiles_all.size();
+                    if (x0 >= 3 && y0 >= 3 && x0 + tx + 3 <= h.nx && y0 + ty + 3 <= h.ny) {
+                        bool simple = true;
+                        for (int y = y0 - 3; y < y0 + ty + 3 && simple; ++y)
+                            for (int x = x0 - 3; x < x0 + tx + 3; ++x)
+                                if (flags_host[p.node_off + (long long)y * p.pitch + x] != 0) { simple = false; break; }
+                        if (simple) gid |= TILE_SIMPLE;
+                    }
+                    const Tile t{(int)k, x0, y0, gid};
+                    tiles_all.push_back(t);
+                    tiles_by_rk[h.rk].push_back(t);
+                    if (h.rk == 1) tiles_rk3.push_back(t);
+                }
+            p.ntile = (int)tiles_all.size() - p.first_tile;
+            tile_first.push_back(p.first_tile);
+            tile_count.push_back(p.ntile);
+        }
+    }
+
+    void upload_tiles()
+    {
+        d_sp.upload(sp, stream);
+        d_tiles_all.upload(tiles_all, stream);
+        d_tiles_rk3.upload(tiles_rk3, stream);
+        for (int m = 0; m < 4; ++m) d_tiles_by_rk[m].upload(tiles_by_rk[m], stream);
+        d_tile_first.upload(tile_first, stream);
+        d_tile_count.upload(tile_count, stream);
+        partial.alloc(tiles_all.size());
+    }
+
+    // TMA descriptors: per sample and stage buffer, the 26 planes as a 3D
+    // tensor (x, y, plane) with the staged halo box of the flux kernels
+    void make_maps()
+    {
+        auto enc = tensor_map_encoder();
+        const int n = (int)hs.size();
+        std::vector<CUtensorMap> maps(2 * n);
+        const size_t es = elem();
+        for (int k = 0; k < n; ++k)
+            for (int b = 0; b < 2; ++b) {
+                unsigned char *base = (b == 0 ? buf2.p : buf3.p) + (size_t)sp[k].state_off * es;
+                cuuint64_t dims[3] = {(cuuint64_t)sp[k].nx, (cuuint64_t)sp[k].ny, (cuuint64_t)NPL};
+                cuuint64_t strides[2] = {(cuuint64_t)sp[k].pitch * es, (cuuint64_t)sp[k].plane * es};
+                cuuint32_t box[3] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 6), 1};
+                cuuint32_t estr[3] = {1, 1, 1};
+                CUresult r = enc(&maps[2 * k + b],
+                                 prec == LBM_PREC_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                                 base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                if (r != CUDA_SUCCESS) throw LbmError(LBM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+            }
+        d_maps.upload(maps, stream);
+    }
+
+    static void check_tile(int x, int y)
+    {
+        if (x * y > 256 || x < 4 || y < 1 || x * y % 32 != 0 || x % 4 != 0 || y + 6 > 256)
+            throw LbmError(LBM_ERR_INVALID, "tile must hold a multiple of 32 and at most 256 nodes, width a multiple of 4");
+    }
+
+    void drop_graphs()
+    {
+        for (auto &g : graph)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+
+    // switch the tile shape: new tile lists and TMA boxes, no state change
+    void retile(int ntx, int nty)
+    {
+        check_tile(ntx, nty);
+        CU(cudaStreamSynchronize(stream));
+        tx = ntx;
+        ty = nty;
+        make_tiles();
+        upload_tiles();
+        make_maps();
+        drop_graphs();
+        CU(cudaStreamSynchronize(stream));
+    }
+
+    // Autotuner: time `steps` steps for each candidate tile shape (CUDA
+    // events, no graph) starting from the same saved state, keep the fastest
+    // and restore the state, so tuning leaves the results unchanged.
+    void autotune(const int *cand, int ncand, int steps, int *chosen, double *ms_out)
+    {
+        if (ncand < 1 || !cand || steps < 1) throw LbmError(LBM_ERR_INVALID, "no tile candidates");
+        for (int c = 0; c < ncand; ++c) check_tile(cand[2 * c], cand[2 * c + 1]);
+        DevBuf<unsigned char> save;
+        save.alloc(state.n);
+        CU(cudaMemcpyAsync(save.p, state.p, state.n, cudaMemcpyDeviceToDevice, stream));
+        std::vector<int> keep_status(host_status);
+        std::vector<HostSample> keep_hs_steps(0);
+        double best = INFINITY;
+        int bx = tx, by = ty;
+        for (int c = 0; c < ncand; ++c) {
+            retile(cand[2 * c], cand[2 * c + 1]);
+            CU(cudaMemcpyAsync(state.p, save.p, state.n, cudaMemcpyDeviceToDevice, stream));
+            double ph[6];
+            profile(1, ph, 6);  // warm-up (module load, caches)
+            CU(cudaMemcpyAsync(state.p, save.p, state.n, cudaMemcpyDeviceToDevice, stream));
+            profile(steps, ph, 6);
+            double tot = 0;
+            for (double v : ph) tot += v;
+            if (ms_out) ms_out[c] = tot;
+            if (tot < best) { best = tot; bx = cand[2 * c]; by = cand[2 * c + 1]; }
+        }
+        retile(bx, by);
+        CU(cudaMemcpyAsync(state.p, save.p, state.n, cudaMemcpyDeviceToDevice, stream));
+        CU(cudaMemsetAsync(status.p, 0, hs.size() * sizeof(int), stream));
+        CU(cudaStreamSynchronize(stream));
+        host_status = keep_status;
+        if (chosen) { chosen[0] = bx; chosen[1] = by; }
     }
 
     template <class S>
@@ -315,8 +448,7 @@ struct lbm_batch {
         if (prec != LBM_PREC_F64 && prec != LBM_PREC_F32) throw LbmError(LBM_ERR_INVALID, "unknown precision");
         if (opt && opt->tile_x > 0) tx = opt->tile_x;
         if (opt && opt->tile_y > 0) ty = opt->tile_y;
-        if (tx * ty > 256 || tx < 4 || ty < 1 || tx * ty % 32 != 0 || tx % 4 != 0)
-            throw LbmError(LBM_ERR_INVALID, "tile must hold a multiple of 32 and at most 256 nodes, width a multiple of 4");
+        check_tile(tx, ty);
         use_graph = opt ? opt->use_graph != 0 : true;
         hs.reserve(n);
         for (int k = 0; k < n; ++k) hs.push_back(derive(cfgs[k], inits[k]));
@@ -408,26 +540,6 @@ struct lbm_batch {
                     if (y < 2 || y > h.ny - 3) fl |= (h.flags & SF_PERY) ? NF_WRPY : NF_EDGY;
                     flags[p.node_off + (long long)y * p.pitch + x] = fl;
                 }
-            // tiles
-            p.first_tile = (int)tiles_all.size();
-            for (int y0 = 0; y0 < h.ny; y0 += ty)
-                for (int x0 = 0; x0 < h.nx; x0 += tx) {
-                    int gid = (int)tiles_all.size();
-                    if (x0 >= 3 && y0 >= 3 && x0 + tx + 3 <= h.nx && y0 + ty + 3 <= h.ny) {
-                        bool simple = true;
-                        for (int y = y0 - 3; y < y0 + ty + 3 && simple; ++y)
-                            for (int x = x0 - 3; x < x0 + tx + 3; ++x)
-                                if (flags[p.node_off + (long long)y * p.pitch + x] != 0) { simple = false; break; }
-                        if (simple) gid |= TILE_SIMPLE;
-                    }
-                    Tile t{k, x0, y0, gid};
-                    tiles_all.push_back(t);
-                    tiles_by_rk[h.rk].push_back(t);
-                    if (h.rk == 1) tiles_rk3.push_back(t);
-                }
-            p.ntile = (int)tiles_all.size() - p.first_tile;
-            tile_first.push_back(p.first_tile);
-            tile_count.push_back(p.ntile);
             // wall nodes: solid with a non-solid 4-neighbour (wallFluxes' test)
             static const int wx[4] = {-1, 1, 0, 0}, wy[4] = {0, 0, -1, 1};
             for (int y = 0; y < h.ny; ++y)
@@ -449,6 +561,8 @@ struct lbm_batch {
         }
         total_state = state_off;
         total_nodes = node_off;
+        flags_host.swap(flags);
+        make_tiles();
 
         state.alloc(total_state * elem());
         buf2.alloc(total_state * elem());
@@ -458,9 +572,8 @@ struct lbm_batch {
         CU(cudaMemsetAsync(buf2.p, 0, buf2.n, stream));
         CU(cudaMemsetAsync(buf3.p, 0, buf3.n, stream));
         CU(cudaMemsetAsync(alpha.p, 0, alpha.n, stream));
-        nflags.upload(flags, stream);
+        nflags.upload(flags_host, stream);
         told.alloc(total_nodes);
-        partial.alloc(tiles_all.size());
         residual.alloc(n);
         status.alloc(n);
         CU(cudaMemsetAsync(status.p, 0, n * sizeof(int), stream));
@@ -468,41 +581,15 @@ struct lbm_batch {
         tdy.upload(v_tdy, stream);
         dxv.upload(v_dx, stream);
         dyv.upload(v_dy, stream);
-        d_sp.upload(sp, stream);
         d_fref.upload(fref_host, stream);
-        d_tiles_all.upload(tiles_all, stream);
-        d_tiles_rk3.upload(tiles_rk3, stream);
-        for (int m = 0; m < 4; ++m) d_tiles_by_rk[m].upload(tiles_by_rk[m], stream);
+        upload_tiles();
         d_walls_all.upload(walls_all, stream);
         d_walls_rk3.upload(walls_rk3, stream);
-        d_tile_first.upload(tile_first, stream);
-        d_tile_count.upload(tile_count, stream);
         scratch.alloc(std::max<size_t>(5 * max_nodes, 2 * 13 * max_nodes));
         host_status.assign(n, 0);
         host_residual.assign(n, 1.0);
 
-        // TMA descriptors: per sample and stage buffer, the 26 planes as a 3D
-        // tensor (x, y, plane) with the staged halo box of the flux kernels
-        {
-            auto enc = tensor_map_encoder();
-            std::vector<CUtensorMap> maps(2 * n);
-            const size_t es = elem();
-            for (int k = 0; k < n; ++k)
-                for (int b = 0; b < 2; ++b) {
-                    unsigned char *base = (b == 0 ? buf2.p : buf3.p) + (size_t)sp[k].state_off * es;
-                    cuuint64_t dims[3] = {(cuuint64_t)sp[k].nx, (cuuint64_t)sp[k].ny, (cuuint64_t)NPL};
-                    cuuint64_t strides[2] = {(cuuint64_t)sp[k].pitch * es, (cuuint64_t)sp[k].plane * es};
-                    cuuint32_t box[3] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 6), 1};
-                    cuuint32_t estr[3] = {1, 1, 1};
-                    CUresult r = enc(&maps[2 * k + b],
-                                     prec == LBM_PREC_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                                     3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-                    if (r != CUDA_SUCCESS) throw LbmError(LBM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-                }
-            d_maps.upload(maps, stream);
-        }
+        make_maps();
         if (prec == LBM_PREC_F64) CU((prepare_kernels<double, double>()));
         else CU((prepare_kernels<float, float>()));
 
@@ -954,6 +1041,21 @@ lbm_status lbm_batch_profile(lbm_batch *b, int n_steps, double *phase_ms, int n_
     if (!b || !phase_ms || n_steps < 1) throw LbmError(LBM_ERR_INVALID, "bad argument");
     b->profile(n_steps, phase_ms, n_phases);
     for (auto &s : b->hs) s.step += n_steps;
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_batch_autotune(lbm_batch *b, const int *candidates, int n_candidates, int steps, int *chosen,
+                              double *ms_per_step)
+{
+    API_BEGIN
+    if (!b) throw LbmError(LBM_ERR_INVALID, "null batch");
+    static const int defaults[] = {16, 16, 32, 8, 64, 4, 8, 32, 32, 4, 16, 8};
+    if (!candidates || n_candidates <= 0) {
+        candidates = defaults;
+        n_candidates = 6;
+    }
+    b->autotune(candidates, n_candidates, steps, chosen, ms_per_step);
     return LBM_OK;
     API_END
 }

@@ -315,7 +315,10 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
     const C c = (C)sp.c;
     const C aex = C(abs(EX)) * c, aey = C(abs(EY)) * c;
     const int nx_items = SX ? 2 * k.TY : 0, ny_items = SY ? 2 * k.TX : 0;
-    const int r = k.tid - ring0;
+    // ring items of this direction start at thread ring0 (0 <= ring0 < NT)
+    // and cover every item even when a group has more items than threads
+    int r0 = k.tid - ring0;
+    if (r0 < 0) r0 += NT;
     if (SIMPLE) {
         // every node fluid and fast-path, every upwind neighbour in the box
         const int lx = k.tx + HALO_X, ly = k.ty + HALO_Y;
@@ -329,14 +332,16 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
             sf[2 * NT + k.tid] = box_flux<S, C>(sp, cf, SY * k.BW, aey);
             sf[3 * NT + k.tid] = box_flux<S, C>(sp, ch, SY * k.BW, aey);
         }
-        if (r >= 0 && r < nx_items) {
-            const int fh = r / k.TY, row = r % k.TY;
-            const int bx = (SX > 0 ? -1 : k.TX) + HALO_X, by = row + HALO_Y;
-            ringx[fh * k.TY + row] = box_flux<S, C>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SX, aex);
-        } else if (r >= nx_items && r < nx_items + ny_items) {
-            const int q = r - nx_items, fh = q / k.TX, col = q % k.TX;
-            const int bx = col + HALO_X, by = (SY > 0 ? -1 : k.TY) + HALO_Y;
-            ringy[fh * k.TX + col] = box_flux<S, C>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SY * k.BW, aey);
+        for (int r = r0; r < nx_items + ny_items; r += NT) {
+            if (r < nx_items) {
+                const int fh = r / k.TY, row = r % k.TY;
+                const int bx = (SX > 0 ? -1 : k.TX) + HALO_X, by = row + HALO_Y;
+                ringx[fh * k.TY + row] = box_flux<S, C>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SX, aex);
+            } else {
+                const int q = r - nx_items, fh = q / k.TX, col = q % k.TX;
+                const int bx = col + HALO_X, by = (SY > 0 ? -1 : k.TY) + HALO_Y;
+                ringy[fh * k.TX + col] = box_flux<S, C>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SY * k.BW, aey);
+            }
         }
         return;
     }
@@ -380,28 +385,30 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
         }
     }
     // upwind neighbours outside the tile: index(x, -e) with reflection
-    if (r >= 0 && r < nx_items) {
-        const int fh = r / k.TY, row = r % k.TY, yy = k.y0 + row;
-        C val = C(0);
-        if (yy < k.y_end) {
-            int m;
-            const int xn = SX > 0 ? k.x0 : k.x_end - 1;
-            const int xr = bc_index(sp, xn, -SX, 0, m);
-            const bool in_box = !m && xr == xn - SX;
-            val = any_node_flux<S, C>(k, box, i, xr, yy, fh, 0, m != 0, in_box);
+    for (int r = r0; r < nx_items + ny_items; r += NT) {
+        if (r < nx_items) {
+            const int fh = r / k.TY, row = r % k.TY, yy = k.y0 + row;
+            C val = C(0);
+            if (yy < k.y_end) {
+                int m;
+                const int xn = SX > 0 ? k.x0 : k.x_end - 1;
+                const int xr = bc_index(sp, xn, -SX, 0, m);
+                const bool in_box = !m && xr == xn - SX;
+                val = any_node_flux<S, C>(k, box, i, xr, yy, fh, 0, m != 0, in_box);
+            }
+            ringx[fh * k.TY + row] = val;
+        } else {
+            const int q = r - nx_items, fh = q / k.TX, col = q % k.TX, xx = k.x0 + col;
+            C val = C(0);
+            if (xx < k.x_end) {
+                int m;
+                const int yn = SY > 0 ? k.y0 : k.y_end - 1;
+                const int yr = bc_index(sp, yn, -SY, 1, m);
+                const bool in_box = !m && yr == yn - SY;
+                val = any_node_flux<S, C>(k, box, i, xx, yr, fh, 1, m != 0, in_box);
+            }
+            ringy[fh * k.TX + col] = val;
         }
-        ringx[fh * k.TY + row] = val;
-    } else if (r >= nx_items && r < nx_items + ny_items) {
-        const int q = r - nx_items, fh = q / k.TX, col = q % k.TX, xx = k.x0 + col;
-        C val = C(0);
-        if (xx < k.x_end) {
-            int m;
-            const int yn = SY > 0 ? k.y0 : k.y_end - 1;
-            const int yr = bc_index(sp, yn, -SY, 1, m);
-            const bool in_box = !m && yr == yn - SY;
-            val = any_node_flux<S, C>(k, box, i, xx, yr, fh, 1, m != 0, in_box);
-        }
-        ringy[fh * k.TX + col] = val;
     }
 }
 
@@ -475,6 +482,7 @@ __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
         C *ry = k.ringy + (size_t)(buf * G + m) * 2 * k.TX;
         dir_fluxes<S, C, SIMPLE>(k, i, boxes + (size_t)(2 * m) * k.pstride, sf, rx, ry, ring0);
         ring0 += (c_EX[i] ? 2 * k.TY : 0) + (c_EY[i] ? 2 * k.TX : 0);
+        while (ring0 >= NT) ring0 -= NT;
     }
     __syncthreads();
     // every thread is done with this slot: refill it NST groups ahead

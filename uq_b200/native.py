@@ -85,6 +85,7 @@ SIGNATURES = {
     "lbm_batch_set_macro": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]),
     "lbm_batch_profile": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int]),
     "lbm_batch_launches_per_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "lbm_batch_autotune": (C.c_int, [C.c_void_p, _ip, C.c_int, C.c_int, _ip, _dp]),
     "lbm_batch_nodes": (C.c_longlong, [C.c_void_p]),
     "lbm_batch_stream": (C.c_void_p, [C.c_void_p]),
     "lbm_batch_destroy": (None, [C.c_void_p]),

@@ -258,5 +258,17 @@ class Batch:
         N.check(N.lib().lbm_batch_profile(self._h, int(n), _d(ms), 6), "lbm_batch_profile")
         return ms
 
+    def autotune(self, candidates=None, steps=2):
+        """Pick the fastest tile shape for this batch (state unchanged);
+        returns ((tile_x, tile_y), {candidate: ms per step})."""
+        if candidates is None:
+            candidates = [(16, 16), (32, 8), (64, 4), (8, 32), (32, 4), (16, 8)]
+        flat = np.array([v for c in candidates for v in c], dtype=np.int32)
+        chosen = np.zeros(2, dtype=np.int32)
+        ms = np.zeros(len(candidates))
+        N.check(N.lib().lbm_batch_autotune(self._h, flat.ctypes.data_as(_ip), len(candidates), int(steps),
+                                           chosen.ctypes.data_as(_ip), _d(ms)), "lbm_batch_autotune")
+        return (int(chosen[0]), int(chosen[1])), {tuple(c): float(t) for c, t in zip(candidates, ms)}
+
     def launches_per_step(self, residual=False):
         return N.lib().lbm_batch_launches_per_step(self._h, 1 if residual else 0)
