@@ -42,7 +42,8 @@ typedef enum lbm_status {
     LBM_ERR_NONFINITE = 5,   /* the state became NaN/Inf or rho <= 0 */
     LBM_ERR_BUSY = 6,        /* serving: queue full / no capacity */
     LBM_ERR_NOT_FOUND = 7,   /* serving: unknown request id */
-    LBM_ERR_TIMEOUT = 8      /* a bounded wait ran out */
+    LBM_ERR_TIMEOUT = 8,     /* a bounded wait ran out */
+    LBM_ERR_CANCELLED = 9    /* serving: the request was cancelled */
 } lbm_status;
 
 /* Storage/compute precision of a handle or batch. */
@@ -183,6 +184,88 @@ LBM_API int lbm_batch_launches_per_step(lbm_batch *b, int want_residual);
 LBM_API long long lbm_batch_nodes(lbm_batch *b);
 LBM_API void *lbm_batch_stream(lbm_batch *b);
 LBM_API void lbm_batch_destroy(lbm_batch *b);
+
+/* ------------------------------------------------------------- serving
+ * No single counterpart in the reference, whose driver runs one solve per
+ * process (main.cpp:32-112).  A server owns a device arena carved from the
+ * free HBM when it is created and a thread that runs solves submitted at
+ * any time, as a continuous batch:
+ *   - a submitted solve waits in a FIFO queue until a region of the arena
+ *     large enough for its f, h and stage buffers is free, then joins the
+ *     resident set at the next step boundary;
+ *   - every step advances all resident solves with one launch per phase
+ *     over their packed tile lists (the launches of lbm_batch_step);
+ *   - at each step boundary finished, failed and cancelled solves leave,
+ *     queued ones join, and the tile lists are repacked; when the arena is
+ *     fragmented the resident regions are moved together first;
+ *   - a finished solve's rho, ux, uy, T, p are copied to host memory by a
+ *     second thread and its region is freed for the queue.
+ * Each solve runs the same per-node arithmetic as alone in a batch of one
+ * with the same precision and tile shape, so its result does not depend on
+ * what else was resident.  The step count of a solve is its derived
+ * nsteps (steps, tt_tref or tt_time of lbm_config); a residual tolerance
+ * alone is not accepted.  A solve whose state fails a device check
+ * (equilibrium mass, non-finite values) is removed within status_poll_steps
+ * steps and completes with that status; the others are not affected. */
+typedef struct lbm_server lbm_server;
+
+typedef struct lbm_server_options {
+    int precision;        /* LBM_PREC_F64 / LBM_PREC_F32, all solves */
+    int tile_x, tile_y;   /* 0: 16 x 16 */
+    size_t arena_bytes;   /* device memory for resident solves; 0: hbm_fraction of the free memory */
+    double hbm_fraction;  /* used when arena_bytes is 0; 0: 0.6 */
+    int max_resident;     /* most solves resident at once; 0: 1024 */
+    int max_queued;       /* most solves waiting; 0: no limit */
+    int use_graph;        /* replay steps from a CUDA graph while the resident set is unchanged */
+    int status_poll_steps;/* steps between reads of the device status words; 0: 32 */
+} lbm_server_options;
+
+enum { LBM_REQ_QUEUED = 0, LBM_REQ_RESIDENT = 1, LBM_REQ_DONE = 2 };
+
+typedef struct lbm_request_info {
+    long long id;
+    int Nx, Ny;
+    int steps_total, steps_done;
+    int state;           /* LBM_REQ_* */
+    lbm_status status;   /* of the finished solve */
+    double t_submit, t_admit, t_done;    /* seconds since the server was created */
+    long long step_admit, step_done;     /* server step count at admission / retirement */
+} lbm_request_info;
+
+typedef struct lbm_server_stats {
+    long long submitted, admitted, completed, failed, cancelled;
+    long long steps;            /* server steps (each advances every resident solve) */
+    long long lattice_updates;  /* sum over steps of the resident nodes */
+    long long repacks, compactions, graph_captures;
+    int resident, queued;
+    long long arena_nodes, arena_nodes_used;
+    size_t arena_bytes;
+    double busy_seconds;        /* wall time with at least one resident solve */
+    double uptime_seconds;
+} lbm_server_stats;
+
+LBM_API lbm_status lbm_server_create(const lbm_server_options *opt, lbm_server **out);
+/* Queue one solve (the arguments of lbm_create).  The host-side set-up
+ * (derived parameters, node flags, tiles) runs on the calling thread.
+ * LBM_ERR_NOMEM: it can never fit the arena; LBM_ERR_BUSY: the queue is full. */
+LBM_API lbm_status lbm_server_submit(lbm_server *s, const lbm_config *cfg, const lbm_init *init, long long *id);
+/* Wait until the solve is done (timeout_s < 0: no limit); LBM_ERR_TIMEOUT
+ * when the time ran out first. */
+LBM_API lbm_status lbm_server_wait(lbm_server *s, long long id, double timeout_s);
+/* Wait for the next solve to finish that no earlier call returned. */
+LBM_API lbm_status lbm_server_wait_any(lbm_server *s, double timeout_s, long long *id);
+LBM_API lbm_status lbm_server_info(lbm_server *s, long long id, lbm_request_info *info);
+/* Copy a finished solve's fields ([x*Ny + y], any pointer may be NULL) and
+ * return its status; LBM_ERR_BUSY while it is not done. */
+LBM_API lbm_status lbm_server_result(lbm_server *s, long long id, double *rho, double *ux, double *uy, double *T,
+                                     double *p);
+/* Cancel a queued or resident solve; it completes with LBM_ERR_CANCELLED. */
+LBM_API lbm_status lbm_server_cancel(lbm_server *s, long long id);
+/* Forget a solve and its result (cancelling it when not done). */
+LBM_API lbm_status lbm_server_release(lbm_server *s, long long id);
+LBM_API lbm_status lbm_server_get_stats(lbm_server *s, lbm_server_stats *st);
+/* Stop the threads; solves not done are dropped. */
+LBM_API void lbm_server_destroy(lbm_server *s);
 
 /* ------------------------------------------------- allocation-free step
  * No counterpart in the reference.  For callers that cannot call

@@ -7,10 +7,7 @@
 // Derived run parameters follow cpuLBM::refineInput / setupVars
 // (CODE/C++/VS2010/simLB/simLB/cpuLBM.cpp:283-450) and the step driver
 // follows runSimStep (main.cpp:32-112).
-#include "lbm_device.cuh"
-#include "lbm_kernels.h"
-#include "lbm_host.h"
-#include "../../include/uq_lbm.h"
+#include "lbm_common.h"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -29,46 +26,6 @@
 namespace uqlbm {
 
 thread_local std::string g_last_error;
-
-template <class T>
-struct DevBuf {
-    T *p = nullptr;
-    size_t n = 0;
-    void alloc(size_t count)
-    {
-        free();
-        if (count == 0) return;
-        CU(cudaMalloc(&p, count * sizeof(T)));
-        n = count;
-    }
-    void upload(const std::vector<T> &v, cudaStream_t s)
-    {
-        alloc(v.size());
-        if (!v.empty()) CU(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
-    }
-    void free()
-    {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    ~DevBuf() { free(); }
-};
-
-// Host-side description of one sample after refineInput / setupVars.
-struct HostSample {
-    int nx = 0, ny = 0, rk = 1, fm = 1;
-    int flags = 0;
-    double R = 1, b = 5, K = 3, Tc = 1, c = 1, mu = 0, Pr = 1, dt = 0, tol = 0;
-    double rho_ref = 1, T_ref = 1;  // completed reference state (refineInput)
-    int nsteps = 0;
-    std::vector<double> dx, dy;
-    std::vector<uint8_t> type;  // [y*nx + x]
-    std::vector<double> rho0, ux0, uy0, T0;  // [y*nx + x] initial node state
-    // driver state (cpuLBM::step, residual, initRes, resNorm; main.cpp:34-70)
-    int step = 0;
-    double residual = 1, resNorm = 0, initRes[100] = {0};
-};
 
 static int host_bc_index(const HostSample &s, int i, int pm, int axis, int &mir)
 {
@@ -137,7 +94,7 @@ void derive_scalars(const lbm_config &c, int Nx, int Ny, double min_spacing, Sca
     if (need) s.nsteps = (int)std::ceil(ttotal / s.dt);
 }
 
-static HostSample derive(const lbm_config &c, const lbm_init &in)
+HostSample derive(const lbm_config &c, const lbm_init &in)
 {
     HostSample s;
     if (!in.bndArray || !in.cellType || !in.density || !in.pressure || !in.temp || !in.velocityX || !in.velocityY ||
@@ -219,7 +176,7 @@ static HostSample derive(const lbm_config &c, const lbm_init &in)
     return s;
 }
 
-static int round_up(int v, int m) { return (v + m - 1) / m * m; }
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against libcuda needed).
@@ -235,6 +192,144 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
         fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
     }
     return fn;
+}
+
+void check_tile_shape(int x, int y)
+{
+    if (x * y > 256 || x < 4 || y < 1 || x * y % 32 != 0 || x % 4 != 0 || y + 6 > 256)
+        throw LbmError(LBM_ERR_INVALID, "tile must hold a multiple of 32 and at most 256 nodes, width a multiple of 4");
+}
+
+// Sample parameters, rest state, node flags, wall list and spacing tables
+// of one sample; layout per sample: 26 planes of ny x pitch, pitch a
+// multiple of 32.
+void prepare_sample(const HostSample &h, int prec, PreparedSample &out)
+{
+    SampleParams &p = out.p;
+    p = SampleParams{};
+    p.nx = h.nx;
+    p.ny = h.ny;
+    p.pitch = round_up(h.nx, 32);
+    p.flags = h.flags;
+    p.rk = h.rk;
+    p.fm = h.fm;
+    p.plane = (long long)p.ny * p.pitch;
+    p.R = h.R;
+    p.bR = h.b * h.R;
+    p.K = h.K;
+    p.Tc = h.Tc;
+    p.inv_sRTc = 1.0 / std::sqrt(h.R * h.Tc);
+    p.RTc = h.R * h.Tc;
+    p.mu = h.mu;
+    p.Pr = h.Pr;
+    p.dt = h.dt;
+    p.c = h.c;
+    p.inv_mu = 1.0 / h.mu;
+    p.two_over_bR = 2.0 / (h.b * h.R);
+    // rest state of the stored deviations (FP32 path only)
+    if (prec == LBM_PREC_F32) {
+        p.rho0 = (h.rho_ref > 0 && std::isfinite(h.rho_ref)) ? h.rho_ref : 1.0;
+        p.T0n = (h.T_ref > 0 && std::isfinite(h.T_ref)) ? h.T_ref / h.Tc : 1.0;
+    } else {
+        p.rho0 = 0.0;
+        p.T0n = 1.0;
+    }
+    {
+        // equilibria at rest per family (the polynomials at u = v = 0)
+        const double T = p.T0n, K = h.K;
+        const double P0[4] = {1 + 2.5 * T * T - 2.5 * T, -T * T + 2.0 * T / 3.0, 0.25 * T * T,
+                              0.125 * T * T - T / 24.0};
+        const double Q0[4] = {T * T * T * (1.25 * K + 20.0 / 3.0) + T * T * (-1.25 * K - 5) + T * (0.5 * K + 1),
+                              T * T * T * (-0.5 * K - 8.0 / 3.0) + T * T * (K / 3.0 + 4.0 / 3.0),
+                              T * T * T * (K / 8.0 + 2.0 / 3.0),
+                              T * T * T * (K / 16.0 + 1.0 / 3.0) + T * T * (-K / 48.0 - 1.0 / 12.0)};
+        double sh = 0;
+        for (int i = 0; i < NQ; ++i) {
+            const int fam = i == 0 ? 0 : (i <= 4 ? 1 : (i <= 8 ? 2 : 3));
+            out.fref[i] = p.rho0 * P0[fam];
+        }
+        for (int i = 0; i < NQ; ++i) {
+            const int fam = i == 0 ? 0 : (i <= 4 ? 1 : (i <= 8 ? 2 : 3));
+            const double hv = p.rho0 * h.R * h.Tc * Q0[fam];
+            out.fref[NQ + i] = hv;
+            sh += hv;
+        }
+        p.shref = sh;
+    }
+    out.tdx.resize(h.nx);
+    out.dx.resize(h.nx);
+    out.tdy.resize(h.ny);
+    out.dy.resize(h.ny);
+    for (int x = 0; x < h.nx; ++x) { out.tdx[x] = h.dt / h.dx[x]; out.dx[x] = h.dx[x]; }
+    for (int y = 0; y < h.ny; ++y) { out.tdy[y] = h.dt / h.dy[y]; out.dy[y] = h.dy[y]; }
+    // node flags
+    out.flags.assign((size_t)p.plane, 0);
+    int m;
+    for (int y = 0; y < h.ny; ++y)
+        for (int x = 0; x < h.nx; ++x) {
+            uint8_t fl = h.type[(size_t)y * h.nx + x];
+            for (int d = -2; d <= 2; ++d) {
+                const int xr = host_bc_index(h, x, d, 0, m);
+                const int yr = host_bc_index(h, y, d, 1, m);
+                if (h.type[(size_t)y * h.nx + xr] == 2) fl |= NF_SOLX;
+                if (h.type[(size_t)yr * h.nx + x] == 2) fl |= NF_SOLY;
+            }
+            if (x < 2 || x > h.nx - 3) fl |= (h.flags & SF_PERX) ? NF_WRPX : NF_EDGX;
+            if (y < 2 || y > h.ny - 3) fl |= (h.flags & SF_PERY) ? NF_WRPY : NF_EDGY;
+            out.flags[(size_t)y * p.pitch + x] = fl;
+        }
+    // wall nodes: solid with a non-solid 4-neighbour (wallFluxes' test)
+    static const int wx[4] = {-1, 1, 0, 0}, wy[4] = {0, 0, -1, 1};
+    out.walls.clear();
+    for (int y = 0; y < h.ny; ++y)
+        for (int x = 0; x < h.nx; ++x) {
+            if (h.type[(size_t)y * h.nx + x] != 2) continue;
+            bool adj = false;
+            for (int j = 0; j < 4; ++j) {
+                const int xm = host_bc_index(h, x, wx[j], 0, m);
+                const int ym = host_bc_index(h, y, wy[j], 1, m);
+                if (h.type[(size_t)ym * h.nx + xm] < 2) adj = true;
+            }
+            if (adj) out.walls.push_back(WallNode{0, x, y, 0});
+        }
+}
+
+// Tiles of one sample, each flagged simple when it and its 3-node halo lie
+// inside the domain and hold only plain fluid nodes.
+void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, int sample, std::vector<Tile> &out)
+{
+    for (int y0 = 0; y0 < ny; y0 += ty)
+        for (int x0 = 0; x0 < nx; x0 += tx) {
+            int gid = (int)out.size();
+            if (x0 >= 3 && y0 >= 3 && x0 + tx + 3 <= nx && y0 + ty + 3 <= ny) {
+                bool simple = true;
+                for (int y = y0 - 3; y < y0 + ty + 3 && simple; ++y)
+                    for (int x = x0 - 3; x < x0 + tx + 3; ++x)
+                        if (flags[(long long)y * pitch + x] != 0) { simple = false; break; }
+                if (simple) gid |= TILE_SIMPLE;
+            }
+            out.push_back(Tile{sample, x0, y0, gid});
+        }
+}
+
+// TMA descriptors: a sample's stage buffer 2 and 3, the 26 planes as a 3D
+// tensor (x, y, plane) with the staged halo box of the flux kernels.
+void encode_stage_maps(int prec, const SampleParams &p, unsigned char *buf2, unsigned char *buf3, int tx, int ty,
+                       CUtensorMap *maps2)
+{
+    auto enc = tensor_map_encoder();
+    const size_t es = prec == LBM_PREC_F64 ? 8 : 4;
+    for (int b = 0; b < 2; ++b) {
+        unsigned char *base = (b == 0 ? buf2 : buf3) + (size_t)p.state_off * es;
+        cuuint64_t dims[3] = {(cuuint64_t)p.nx, (cuuint64_t)p.ny, (cuuint64_t)NPL};
+        cuuint64_t strides[2] = {(cuuint64_t)p.pitch * es, (cuuint64_t)p.plane * es};
+        cuuint32_t box[3] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 6), 1};
+        cuuint32_t estr[3] = {1, 1, 1};
+        CUresult r = enc(&maps2[b], prec == LBM_PREC_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) throw LbmError(LBM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    }
 }
 
 }  // namespace uqlbm
@@ -297,22 +392,12 @@ struct lbm_batch {
             const HostSample &h = hs[k];
             SampleParams &p = sp[k];
             p.first_tile = (int)tiles_all.size();
-            for (int y0 = 0; y0 < h.ny; y0 += ty)
-                for (int x0 = 0; x0 < h.nx; x0 += tx) {
-                    int gid = (int)tiles_all.size();
-                    if (x0 >= 3 && y0 >= 3 && x0 + tx + 3 <= h.nx && y0 + ty + 3 <= h.ny) {
-                        bool simple = true;
-                        for (int y = y0 - 3; y < y0 + ty + 3 && simple; ++y)
-                            for (int x = x0 - 3; x < x0 + tx + 3; ++x)
-                                if (flags_host[p.node_off + (long long)y * p.pitch + x] != 0) { simple = false; break; }
-                        if (simple) gid |= TILE_SIMPLE;
-                    }
-                    const Tile t{(int)k, x0, y0, gid};
-                    tiles_all.push_back(t);
-                    tiles_by_rk[h.rk].push_back(t);
-                    if (h.rk == 1) tiles_rk3.push_back(t);
-                }
+            cut_tiles(flags_host.data() + p.node_off, p.pitch, h.nx, h.ny, tx, ty, (int)k, tiles_all);
             p.ntile = (int)tiles_all.size() - p.first_tile;
+            for (int t = p.first_tile; t < p.first_tile + p.ntile; ++t) {
+                tiles_by_rk[h.rk].push_back(tiles_all[t]);
+                if (h.rk == 1) tiles_rk3.push_back(tiles_all[t]);
+            }
             tile_first.push_back(p.first_tile);
             tile_count.push_back(p.ntile);
         }
@@ -333,31 +418,13 @@ struct lbm_batch {
     // tensor (x, y, plane) with the staged halo box of the flux kernels
     void make_maps()
     {
-        auto enc = tensor_map_encoder();
         const int n = (int)hs.size();
         std::vector<CUtensorMap> maps(2 * n);
-        const size_t es = elem();
-        for (int k = 0; k < n; ++k)
-            for (int b = 0; b < 2; ++b) {
-                unsigned char *base = (b == 0 ? buf2.p : buf3.p) + (size_t)sp[k].state_off * es;
-                cuuint64_t dims[3] = {(cuuint64_t)sp[k].nx, (cuuint64_t)sp[k].ny, (cuuint64_t)NPL};
-                cuuint64_t strides[2] = {(cuuint64_t)sp[k].pitch * es, (cuuint64_t)sp[k].plane * es};
-                cuuint32_t box[3] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 6), 1};
-                cuuint32_t estr[3] = {1, 1, 1};
-                CUresult r = enc(&maps[2 * k + b],
-                                 prec == LBM_PREC_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
-                                 base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-                if (r != CUDA_SUCCESS) throw LbmError(LBM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-            }
+        for (int k = 0; k < n; ++k) encode_stage_maps(prec, sp[k], buf2.p, buf3.p, tx, ty, &maps[2 * k]);
         d_maps.upload(maps, stream);
     }
 
-    static void check_tile(int x, int y)
-    {
-        if (x * y > 256 || x < 4 || y < 1 || x * y % 32 != 0 || x % 4 != 0 || y + 6 > 256)
-            throw LbmError(LBM_ERR_INVALID, "tile must hold a multiple of 32 and at most 256 nodes, width a multiple of 4");
-    }
+    static void check_tile(int x, int y) { check_tile_shape(x, y); }
 
     void drop_graphs()
     {
@@ -458,104 +525,34 @@ struct lbm_batch {
         CU(cudaGetDevice(&device));
         CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 
-        // layout: per sample 26 planes of ny x pitch, pitch a multiple of 32
+        // layout: per sample 26 planes of ny x pitch, packed one after another
         std::vector<double> v_tdx, v_tdy, v_dx, v_dy, fref_host;
         std::vector<uint8_t> flags;
         long long state_off = 0, node_off = 0;
+        PreparedSample ps;
         for (int k = 0; k < n; ++k) {
             const HostSample &h = hs[k];
-            SampleParams p{};
-            p.nx = h.nx;
-            p.ny = h.ny;
-            p.pitch = round_up(h.nx, 32);
-            p.flags = h.flags;
-            p.rk = h.rk;
-            p.fm = h.fm;
-            p.plane = (long long)p.ny * p.pitch;
+            prepare_sample(h, prec, ps);
+            SampleParams p = ps.p;
             p.state_off = state_off;
             p.node_off = node_off;
             p.xoff = (int)v_tdx.size();
             p.yoff = (int)v_tdy.size();
-            p.R = h.R;
-            p.bR = h.b * h.R;
-            p.K = h.K;
-            p.Tc = h.Tc;
-            p.inv_sRTc = 1.0 / std::sqrt(h.R * h.Tc);
-            p.RTc = h.R * h.Tc;
-            p.mu = h.mu;
-            p.Pr = h.Pr;
-            p.dt = h.dt;
-            p.c = h.c;
-            p.inv_mu = 1.0 / h.mu;
-            p.two_over_bR = 2.0 / (h.b * h.R);
-            // rest state of the stored deviations (FP32 path only)
-            if (prec == LBM_PREC_F32) {
-                p.rho0 = (h.rho_ref > 0 && std::isfinite(h.rho_ref)) ? h.rho_ref : 1.0;
-                p.T0n = (h.T_ref > 0 && std::isfinite(h.T_ref)) ? h.T_ref / h.Tc : 1.0;
-            } else {
-                p.rho0 = 0.0;
-                p.T0n = 1.0;
+            fref_host.insert(fref_host.end(), ps.fref, ps.fref + NPL);
+            v_tdx.insert(v_tdx.end(), ps.tdx.begin(), ps.tdx.end());
+            v_tdy.insert(v_tdy.end(), ps.tdy.begin(), ps.tdy.end());
+            v_dx.insert(v_dx.end(), ps.dx.begin(), ps.dx.end());
+            v_dy.insert(v_dy.end(), ps.dy.begin(), ps.dy.end());
+            flags.insert(flags.end(), ps.flags.begin(), ps.flags.end());
+            for (WallNode w : ps.walls) {
+                w.sample = k;
+                walls_all.push_back(w);
+                if (h.rk == 1) walls_rk3.push_back(w);
             }
-            {
-                // equilibria at rest per family (the polynomials at u = v = 0)
-                const double T = p.T0n, K = h.K;
-                const double P0[4] = {1 + 2.5 * T * T - 2.5 * T, -T * T + 2.0 * T / 3.0, 0.25 * T * T,
-                                      0.125 * T * T - T / 24.0};
-                const double Q0[4] = {T * T * T * (1.25 * K + 20.0 / 3.0) + T * T * (-1.25 * K - 5) + T * (0.5 * K + 1),
-                                      T * T * T * (-0.5 * K - 8.0 / 3.0) + T * T * (K / 3.0 + 4.0 / 3.0),
-                                      T * T * T * (K / 8.0 + 2.0 / 3.0),
-                                      T * T * T * (K / 16.0 + 1.0 / 3.0) + T * T * (-K / 48.0 - 1.0 / 12.0)};
-                double sh = 0;
-                for (int i = 0; i < NQ; ++i) {
-                    const int fam = i == 0 ? 0 : (i <= 4 ? 1 : (i <= 8 ? 2 : 3));
-                    fref_host.push_back(p.rho0 * P0[fam]);
-                }
-                for (int i = 0; i < NQ; ++i) {
-                    const int fam = i == 0 ? 0 : (i <= 4 ? 1 : (i <= 8 ? 2 : 3));
-                    const double hv = p.rho0 * h.R * h.Tc * Q0[fam];
-                    fref_host.push_back(hv);
-                    sh += hv;
-                }
-                p.shref = sh;
-            }
-            for (int x = 0; x < h.nx; ++x) { v_tdx.push_back(h.dt / h.dx[x]); v_dx.push_back(h.dx[x]); }
-            for (int y = 0; y < h.ny; ++y) { v_tdy.push_back(h.dt / h.dy[y]); v_dy.push_back(h.dy[y]); }
             state_off += NPL * p.plane;
             node_off += p.plane;
             lattice_nodes += (long long)h.nx * h.ny;
             max_nodes = std::max(max_nodes, (size_t)h.nx * h.ny);
-            // node flags
-            flags.resize(node_off, 0);
-            for (int y = 0; y < h.ny; ++y)
-                for (int x = 0; x < h.nx; ++x) {
-                    uint8_t fl = h.type[(size_t)y * h.nx + x];
-                    int m;
-                    for (int d = -2; d <= 2; ++d) {
-                        const int xr = host_bc_index(h, x, d, 0, m);
-                        const int yr = host_bc_index(h, y, d, 1, m);
-                        if (h.type[(size_t)y * h.nx + xr] == 2) fl |= NF_SOLX;
-                        if (h.type[(size_t)yr * h.nx + x] == 2) fl |= NF_SOLY;
-                    }
-                    if (x < 2 || x > h.nx - 3) fl |= (h.flags & SF_PERX) ? NF_WRPX : NF_EDGX;
-                    if (y < 2 || y > h.ny - 3) fl |= (h.flags & SF_PERY) ? NF_WRPY : NF_EDGY;
-                    flags[p.node_off + (long long)y * p.pitch + x] = fl;
-                }
-            // wall nodes: solid with a non-solid 4-neighbour (wallFluxes' test)
-            static const int wx[4] = {-1, 1, 0, 0}, wy[4] = {0, 0, -1, 1};
-            for (int y = 0; y < h.ny; ++y)
-                for (int x = 0; x < h.nx; ++x) {
-                    if (h.type[(size_t)y * h.nx + x] != 2) continue;
-                    bool adj = false;
-                    for (int j = 0; j < 4; ++j) {
-                        const int xm = host_bc_index(h, x, wx[j], 0, m_dummy());
-                        const int ym = host_bc_index(h, y, wy[j], 1, m_dummy());
-                        if (h.type[(size_t)ym * h.nx + xm] < 2) adj = true;
-                    }
-                    if (adj) {
-                        walls_all.push_back(WallNode{k, x, y, 0});
-                        if (h.rk == 1) walls_rk3.push_back(WallNode{k, x, y, 0});
-                    }
-                }
             if (h.rk == 1) any_rk3 = true; else any_other = true;
             sp.push_back(p);
         }
@@ -621,10 +618,20 @@ struct lbm_batch {
         CU(cudaStreamSynchronize(stream));
     }
 
-    static int &m_dummy()
+    StepLists lists() const
     {
-        static thread_local int m;
-        return m;
+        StepLists l;
+        for (int m = 0; m < 4; ++m) {
+            l.by_rk[m] = d_tiles_by_rk[m].p;
+            l.n_by_rk[m] = (int)tiles_by_rk[m].size();
+        }
+        l.rk3 = d_tiles_rk3.p;
+        l.n_rk3 = any_rk3 ? (int)tiles_rk3.size() : 0;
+        l.walls_all = d_walls_all.p;
+        l.n_walls_all = (int)walls_all.size();
+        l.walls_rk3 = d_walls_rk3.p;
+        l.n_walls_rk3 = (int)walls_rk3.size();
+        return l;
     }
 
     // One step.  ev (optional) receives 7 events around the phases:
@@ -633,36 +640,13 @@ struct lbm_batch {
     template <class S, class C>
     void enqueue_step_t(int want_res, cudaEvent_t *ev = nullptr)
     {
-        const KArgs<S> a = args<S>(want_res);
-        if (ev) CU(cudaEventRecord(ev[0], stream));
-        // pointwise stages, per method
-        for (int m = 0; m < 4; ++m)
-            if (!tiles_by_rk[m].empty())
-                CU((launch_phase<S, C>(a, 0, m, d_tiles_by_rk[m].p, (int)tiles_by_rk[m].size(), nullptr, 0, stream)));
-        if (ev) CU(cudaEventRecord(ev[1], stream));
-        CU((launch_phase<S, C>(a, 3, 0, nullptr, 0, d_walls_all.p, (int)walls_all.size(), stream)));
-        if (ev) CU(cudaEventRecord(ev[2], stream));
-        for (int m = 0; m < 4; ++m)
-            if (!tiles_by_rk[m].empty())
-                CU((launch_phase<S, C>(a, 1, m, d_tiles_by_rk[m].p, (int)tiles_by_rk[m].size(), nullptr, 0, stream)));
-        if (ev) CU(cudaEventRecord(ev[3], stream));
-        if (any_rk3) CU((launch_phase<S, C>(a, 4, 1, nullptr, 0, d_walls_rk3.p, (int)walls_rk3.size(), stream)));
-        if (ev) CU(cudaEventRecord(ev[4], stream));
-        if (any_rk3) CU((launch_phase<S, C>(a, 2, 1, d_tiles_rk3.p, (int)tiles_rk3.size(), nullptr, 0, stream)));
-        if (ev) CU(cudaEventRecord(ev[5], stream));
+        enqueue_step_phases<S, C>(args<S>(want_res), lists(), stream, ev);
         if (want_res)
             CU(launch_residual(d_sp.p, (int)hs.size(), partial.p, d_tile_first.p, d_tile_count.p, residual.p, stream));
         if (ev) CU(cudaEventRecord(ev[6], stream));
     }
 
-    int launches_per_step(int want_res) const
-    {
-        int n = 0;
-        for (int m = 0; m < 4; ++m) n += tiles_by_rk[m].empty() ? 0 : 2;  // pointwise + stencil
-        n += walls_all.empty() ? 0 : 1;
-        if (any_rk3) n += (walls_rk3.empty() ? 0 : 1) + 1;
-        return n + (want_res ? 1 : 0);
-    }
+    int launches_per_step(int want_res) const { return step_launches(lists()) + (want_res ? 1 : 0); }
 
     void profile(int n, double *ms, int nph)
     {

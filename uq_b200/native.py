@@ -21,8 +21,10 @@ LBM_ERR_NONFINITE = 5
 LBM_ERR_BUSY = 6
 LBM_ERR_NOT_FOUND = 7
 LBM_ERR_TIMEOUT = 8
+LBM_ERR_CANCELLED = 9
 STATUS_NAMES = {0: "ok", 1: "equilibrium", 2: "invalid", 3: "cuda", 4: "nomem", 5: "nonfinite",
-                6: "busy", 7: "not_found", 8: "timeout"}
+                6: "busy", 7: "not_found", 8: "timeout", 9: "cancelled"}
+LBM_REQ_QUEUED, LBM_REQ_RESIDENT, LBM_REQ_DONE = 0, 1, 2
 
 PREC = {"f64": 0, "f32": 1}
 
@@ -62,6 +64,28 @@ class LbmBatchOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("tile_x", C.c_int), ("tile_y", C.c_int), ("use_graph", C.c_int)]
 
 
+class LbmServerOptions(C.Structure):
+    _fields_ = [("precision", C.c_int), ("tile_x", C.c_int), ("tile_y", C.c_int), ("arena_bytes", C.c_size_t),
+                ("hbm_fraction", C.c_double), ("max_resident", C.c_int), ("max_queued", C.c_int),
+                ("use_graph", C.c_int), ("status_poll_steps", C.c_int)]
+
+
+class LbmRequestInfo(C.Structure):
+    _fields_ = [("id", C.c_longlong), ("Nx", C.c_int), ("Ny", C.c_int), ("steps_total", C.c_int),
+                ("steps_done", C.c_int), ("state", C.c_int), ("status", C.c_int), ("t_submit", C.c_double),
+                ("t_admit", C.c_double), ("t_done", C.c_double), ("step_admit", C.c_longlong),
+                ("step_done", C.c_longlong)]
+
+
+class LbmServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("admitted", C.c_longlong), ("completed", C.c_longlong),
+                ("failed", C.c_longlong), ("cancelled", C.c_longlong), ("steps", C.c_longlong),
+                ("lattice_updates", C.c_longlong), ("repacks", C.c_longlong), ("compactions", C.c_longlong),
+                ("graph_captures", C.c_longlong), ("resident", C.c_int), ("queued", C.c_int),
+                ("arena_nodes", C.c_longlong), ("arena_nodes_used", C.c_longlong), ("arena_bytes", C.c_size_t),
+                ("busy_seconds", C.c_double), ("uptime_seconds", C.c_double)]
+
+
 # name -> (restype, argtypes); every function include/uq_lbm.h declares
 SIGNATURES = {
     "lbm_create": (C.c_int, [C.POINTER(LbmConfig), C.POINTER(LbmInit), C.c_int, C.POINTER(C.c_void_p)]),
@@ -89,6 +113,16 @@ SIGNATURES = {
     "lbm_batch_nodes": (C.c_longlong, [C.c_void_p]),
     "lbm_batch_stream": (C.c_void_p, [C.c_void_p]),
     "lbm_batch_destroy": (None, [C.c_void_p]),
+    "lbm_server_create": (C.c_int, [C.POINTER(LbmServerOptions), C.POINTER(C.c_void_p)]),
+    "lbm_server_submit": (C.c_int, [C.c_void_p, C.POINTER(LbmConfig), C.POINTER(LbmInit), C.POINTER(C.c_longlong)]),
+    "lbm_server_wait": (C.c_int, [C.c_void_p, C.c_longlong, C.c_double]),
+    "lbm_server_wait_any": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_longlong)]),
+    "lbm_server_info": (C.c_int, [C.c_void_p, C.c_longlong, C.POINTER(LbmRequestInfo)]),
+    "lbm_server_result": (C.c_int, [C.c_void_p, C.c_longlong, _dp, _dp, _dp, _dp, _dp]),
+    "lbm_server_cancel": (C.c_int, [C.c_void_p, C.c_longlong]),
+    "lbm_server_release": (C.c_int, [C.c_void_p, C.c_longlong]),
+    "lbm_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(LbmServerStats)]),
+    "lbm_server_destroy": (None, [C.c_void_p]),
     "lbm_step_noalloc": (C.c_int, [C.POINTER(LbmConfig), C.c_int, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_int,
                                    C.c_void_p]),
 }

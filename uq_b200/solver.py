@@ -5,8 +5,9 @@
 MAT variables of ``loadInput``, see ``uq_b200.workloads``), steps with
 ``runOne`` / ``run`` and exposes ``rho_G, u_G, T_G, p_G, f_G, h_G`` in the
 reference's layouts (``macros.h:8-14``).  ``Batch`` advances many samples
-in one launch sequence.  Both run only on the CUDA library; a missing
-library raises.
+in one launch sequence; ``Server`` runs solves submitted at any time as a
+continuous batch.  All run only on the CUDA library; a missing library
+raises.
 """
 import ctypes as C
 
@@ -272,3 +273,83 @@ class Batch:
 
     def launches_per_step(self, residual=False):
         return N.lib().lbm_batch_launches_per_step(self._h, 1 if residual else 0)
+
+
+class Server:
+    """A request server (an ``lbm_server``): solves submitted at any time run
+    as one continuous batch on the GPU; results come back per request."""
+
+    def __init__(self, precision="f32", tile=(0, 0), arena_bytes=0, hbm_fraction=0.0, max_resident=0,
+                 max_queued=0, use_graph=True, status_poll_steps=0):
+        L = N.lib()
+        opt = N.LbmServerOptions(N.PREC[precision], int(tile[0]), int(tile[1]), int(arena_bytes),
+                                 float(hbm_fraction), int(max_resident), int(max_queued), 1 if use_graph else 0,
+                                 int(status_poll_steps))
+        h = C.c_void_p()
+        N.check(L.lbm_server_create(C.byref(opt), C.byref(h)), "lbm_server_create")
+        self._h = h
+        self.precision = precision
+        self._shapes = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().lbm_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, case):
+        """Queue one solve; returns its request id."""
+        b = _CaseBuffers(case)
+        rid = C.c_longlong()
+        N.check(N.lib().lbm_server_submit(self._h, C.byref(b.cfg), C.byref(b.ini), C.byref(rid)),
+                "lbm_server_submit")
+        self._shapes[rid.value] = (b.nx, b.ny)
+        return rid.value
+
+    def wait(self, rid, timeout=-1.0):
+        """True when the request finished, False when the timeout ran out."""
+        code = N.lib().lbm_server_wait(self._h, int(rid), float(timeout))
+        if code == N.LBM_ERR_TIMEOUT:
+            return False
+        N.check(code, "lbm_server_wait")
+        return True
+
+    def wait_any(self, timeout=-1.0):
+        """Id of the next finished request, or None when the timeout ran out."""
+        rid = C.c_longlong()
+        code = N.lib().lbm_server_wait_any(self._h, float(timeout), C.byref(rid))
+        if code == N.LBM_ERR_TIMEOUT:
+            return None
+        N.check(code, "lbm_server_wait_any")
+        return rid.value
+
+    def info(self, rid):
+        i = N.LbmRequestInfo()
+        N.check(N.lib().lbm_server_info(self._h, int(rid), C.byref(i)), "lbm_server_info")
+        return {name: getattr(i, name) for name, _ in N.LbmRequestInfo._fields_}
+
+    def result(self, rid):
+        """(status, fields) of a finished request; fields as ``Solver.macro``."""
+        nx, ny = self._shapes[rid]
+        out = {k: np.empty(nx * ny) for k in ("rho", "ux", "uy", "T", "p")}
+        code = N.lib().lbm_server_result(self._h, int(rid), *[_d(out[k]) for k in ("rho", "ux", "uy", "T", "p")])
+        if code in (N.LBM_ERR_BUSY, N.LBM_ERR_NOT_FOUND, N.LBM_ERR_INVALID):
+            N.check(code, "lbm_server_result")
+        return code, {k: v.reshape(nx, ny) for k, v in out.items()}
+
+    def cancel(self, rid):
+        N.check(N.lib().lbm_server_cancel(self._h, int(rid)), "lbm_server_cancel")
+
+    def release(self, rid):
+        N.check(N.lib().lbm_server_release(self._h, int(rid)), "lbm_server_release")
+        self._shapes.pop(rid, None)
+
+    def stats(self):
+        s = N.LbmServerStats()
+        N.check(N.lib().lbm_server_get_stats(self._h, C.byref(s)), "lbm_server_get_stats")
+        return {name: getattr(s, name) for name, _ in N.LbmServerStats._fields_}
