@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile", default="0,0")
+    ap.add_argument("--serving-seconds", type=float, default=45.0,
+                    help="Poisson arrival window of the serving run (0: skip it)")
     return ap.parse_args()
 
 
@@ -224,6 +226,150 @@ def plain_fp64_probe(samples, steps=10, n=32):
     return lu / wall / 1e6
 
 
+SERVE_SIDES = (32, 1024)      # square grid side ~ U{32..1024}
+SERVE_STEPS = (200, 5000)     # step count ~ U{200..5000}
+
+
+def _serving_requests(seconds, lam, seed):
+    """Poisson(lam) arrivals over `seconds`: Couette or Riemann solves with
+    random side, step count and RK method (RK1/RK3); Couette solves use
+    WENO5 or NND, Riemann solves NND (with WENO5 the Riemann problem
+    reaches the equilibrium failure check within 500-3000 steps at every
+    CFL tried, in FP64 as in FP32)."""
+    rng = np.random.default_rng(seed)
+    reqs, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / lam)
+        if t >= seconds:
+            break
+        kind = ["couette", "riemann"][int(rng.integers(0, 2))]
+        fm = int(rng.integers(0, 2))
+        reqs.append(dict(t=t, kind=kind, side=int(rng.integers(SERVE_SIDES[0], SERVE_SIDES[1] + 1)),
+                         steps=int(rng.integers(SERVE_STEPS[0], SERVE_STEPS[1] + 1)),
+                         fm=fm if kind == "couette" else 0, rk=int(rng.integers(0, 2)),
+                         seed=int(rng.integers(1 << 30))))
+    return reqs
+
+
+def _serving_case(r, steps=None):
+    from uq_b200 import workloads as W
+
+    n = steps if steps is not None else r["steps"]
+    # CFL numbers at which every method combination stays within the
+    # equilibrium check for 5000 steps
+    if r["kind"] == "couette":
+        return W.couette(nx=r["side"], ny=r["side"], steps=n, seed=r["seed"], fmethod=r["fm"], rkmethod=r["rk"],
+                         CFL=0.3)
+    return W.riemann(nx=r["side"], ny=r["side"], steps=n, fmethod=r["fm"], rkmethod=r["rk"], CFL=0.05)
+
+
+def _alone_fp64_rates(sides=(32, 128, 512, 1024), steps=10):
+    """Plain FP64 path (one lbm_handle) MLUPS per (kind, rk, fm, side)."""
+    import torch
+
+    from uq_b200.solver import Solver
+
+    rates = {}
+    for kind in ("couette", "riemann"):
+        for rk in (0, 1):
+            for fm in ((0, 1) if kind == "couette" else (0,)):
+                for side in sides:
+                    s = Solver(_serving_case(dict(kind=kind, side=side, rk=rk, fm=fm, seed=1), steps + 2), "f64")
+                    s.step(2)
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    s.step(steps)
+                    torch.cuda.synchronize()
+                    rates[(kind, rk, fm, side)] = side * side * steps / (time.perf_counter() - t0) / 1e6
+                    s.close()
+    return rates
+
+
+def _alone_rate(rates, r, sides=(32, 128, 512, 1024)):
+    """log-log interpolation of the plain FP64 rate in the grid side."""
+    xs = np.log(np.array(sides, dtype=float))
+    ys = np.log(np.array([rates[(r["kind"], r["rk"], r["fm"], s)] for s in sides]))
+    return float(np.exp(np.interp(np.log(r["side"]), xs, ys)))
+
+
+def serving_probe(seconds, capacity_mlups, load=0.7, seed=4242):
+    """Continuous-batching serving run: Poisson arrivals submitted in real
+    time to one lbm_server (FP32), results collected as they finish.
+    Latency = result in host memory - scheduled arrival.  The same requests
+    run alone one after another on the plain FP64 path would take the sum of
+    their alone times (rates measured per kind/method/side, interpolated)."""
+    import threading
+
+    from uq_b200.solver import Server
+
+    sides = np.arange(SERVE_SIDES[0], SERVE_SIDES[1] + 1, dtype=float)
+    mean_work = float(np.mean(sides ** 2)) * (SERVE_STEPS[0] + SERVE_STEPS[1]) / 2.0
+    lam = load * capacity_mlups * 1e6 / mean_work
+    reqs = _serving_requests(seconds, lam, seed)
+    cases = [_serving_case(r) for r in reqs]
+    srv = Server(precision="f32")
+    warm = srv.submit(_serving_case(dict(kind="couette", side=64, steps=20, fm=1, rk=1, seed=3)))
+    srv.wait(warm)
+    srv.release(warm)
+    ids, t_arrive, t_done, status = {}, {}, {}, {}
+    errors = []
+    t0 = time.perf_counter()
+
+    def submitter():
+        try:
+            for k, (r, c) in enumerate(zip(reqs, cases)):
+                dt = t0 + r["t"] - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids[srv.submit(c)] = k
+                t_arrive[k] = t0 + r["t"]
+        except Exception as exc:  # reported below
+            errors.append(repr(exc))
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    got = 0
+    while got < len(reqs) and not errors:
+        rid = srv.wait_any(timeout=600.0)
+        if rid is None:
+            errors.append("no request finished within 600 s")
+            break
+        code, _ = srv.result(rid)  # copy the fields to host memory
+        t = time.perf_counter()
+        while rid not in ids:  # the submitter records the id right after submit returns
+            time.sleep(1e-4)
+        t_done[ids[rid]] = t
+        status[ids[rid]] = int(code)
+        srv.release(rid)
+        got += 1
+    th.join()
+    t_end = time.perf_counter()
+    st = srv.stats()
+    srv.close()
+    lat = np.array([t_done[k] - t_arrive[k] for k in sorted(t_done)])
+    lu = float(sum(r["side"] ** 2 * r["steps"] for r in reqs))
+    rates = _alone_fp64_rates()
+    alone = np.array([r["side"] ** 2 * r["steps"] / (_alone_rate(rates, r) * 1e6) for r in reqs])
+    done_k = sorted(t_done)
+    return {
+        "requests": len(reqs), "completed_ok": int(sum(1 for v in status.values() if v == 0)),
+        "arrival_rate_per_s": lam, "offered_load": load, "window_s": seconds,
+        "mix": "couette (CFL 0.3, WENO5|NND) | riemann (CFL 0.05, NND), side~U{%d..%d}, steps~U{%d..%d}, "
+               "RK1|RK3, FP32" % (SERVE_SIDES + SERVE_STEPS),
+        "latency_s": {"p50": float(np.percentile(lat, 50)) if lat.size else None,
+                      "p99": float(np.percentile(lat, 99)) if lat.size else None,
+                      "max": float(lat.max()) if lat.size else None},
+        "latency_over_alone_fp64": {
+            "p50": float(np.percentile(lat / alone[done_k], 50)) if lat.size else None,
+            "p99": float(np.percentile(lat / alone[done_k], 99)) if lat.size else None},
+        "aggregate_mlups": lu / (t_end - t0) / 1e6,
+        "busy_mlups": st["lattice_updates"] / max(st["busy_seconds"], 1e-9) / 1e6,
+        "alone_fp64_sequential_mlups": lu / float(alone.sum()) / 1e6,
+        "server": {k: st[k] for k in ("steps", "repacks", "compactions", "graph_captures", "arena_bytes")},
+        "errors": errors,
+    }
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -338,6 +484,14 @@ def run_ours(args, rank, world, local_rank):
         cpu = {"value": v, "unit": "MLUPS", "cores": cores, "kind": kind,
                "sample": "%d processes, each one 64x64 ensemble sample x 20 steps (%.1f s wall)" % (cores, wall)}
 
+    launches = b.launches_per_step(False) * args.steps
+    b.close()
+    if rank == 0 and world == 1 and args.serving_seconds > 0:
+        try:
+            extra["serving"] = serving_probe(args.serving_seconds, value)
+        except Exception as exc:  # reported, not fatal
+            extra["serving"] = {"error": repr(exc)}
+
     if rank == 0:
         out = {
             "metric": "batched f+h MLUPS (UQ ensemble, WENO5 RK3)", "value": value, "unit": "MLUPS",
@@ -357,14 +511,13 @@ def run_ours(args, rank, world, local_rank):
             "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d / args.steps,
                     "d2h_bytes_per_step": d2h / args.steps,
                     "what": "per solve: pinned host fields -> lbm_batch_set_macro, K steps, lbm_batch_get_macro"},
-            "gpu_launches": b.launches_per_step(False) * args.steps,
+            "gpu_launches": launches,
             "clocks": clk,
             "sample_status": {"ok": int((status == 0).sum()), "failed": int((status != 0).sum())},
             "cpu_baseline": cpu,
         }
         out.update(extra)
         print(json.dumps(out), flush=True)
-    b.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -159,3 +159,33 @@ def test_cancel_release_and_errors(cuda_device):
     assert e.value.code == N.LBM_ERR_INVALID
     small.close()
     srv.close()
+
+
+def test_fragmented_arena_is_compacted(cuda_device):
+    # three 64 x 64 solves (4096 node slots each) fill an arena of ~3.6 of
+    # them; the middle one finishes first and leaves a hole too small for a
+    # 96 x 64 solve (6144 slots), although the free total is large enough
+    a = W.couette(nx=64, ny=64, steps=3000, seed=11)
+    b = W.couette(nx=64, ny=64, steps=5, seed=12)
+    c = W.couette(nx=64, ny=64, steps=3000, seed=13, fmethod=0)
+    d = W.couette(nx=96, ny=64, steps=20, seed=14, rkmethod=0)
+    slots = 4096
+    srv = Server(precision="f32", arena_bytes=int(3.6 * slots * BYTES_PER_NODE["f32"]), use_graph=False)
+    ids = [srv.submit(a), srv.submit(b), srv.submit(c)]
+    assert srv.wait(ids[1], timeout=120.0)
+    assert srv.info(ids[0])["state"] == N.LBM_REQ_RESIDENT
+    ids.append(srv.submit(d))
+    for rid in ids:
+        assert srv.wait(rid, timeout=120.0)
+    stats = srv.stats()
+    assert stats["compactions"] >= 1
+    # d was admitted while a and c were still resident
+    info_d, info_a = srv.info(ids[3]), srv.info(ids[0])
+    assert info_d["step_admit"] < info_a["step_done"]
+    for rid, case in zip(ids, (a, b, c, d)):
+        code, got = srv.result(rid)
+        st, ref = _alone(case, "f32")
+        assert code == st == N.LBM_OK
+        for f in FIELDS:
+            assert np.array_equal(got[f], ref[f]), (rid, f)
+    srv.close()

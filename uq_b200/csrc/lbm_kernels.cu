@@ -29,9 +29,35 @@ __device__ __forceinline__ S *plane_ptr(S *base, const SampleParams &sp, int p)
 }
 
 // ------------------------------------------------------------------- init
-// initialiseFunctions (cpuLBM.cpp:846-875): f, h = equilibrium of each
-// node's property; solid and permanent nodes also seed stage buffers 2/3,
-// whose contents never change for them.
+// initialiseFunctions (cpuLBM.cpp:846-875) for one node: f, h = equilibrium
+// of (rho, ux, uy, T), stored as deviations from the rest state; solid and
+// permanent nodes also seed stage buffers 2/3, whose contents never change
+// for them.  Returns false when the equilibrium mass check fails.  One
+// compiled body serves every initialising kernel, so a state set from
+// fields is bit-for-bit the state built at creation.
+template <class S>
+__device__ __noinline__ bool init_node(double rho, double ux, double uy, double T, const SampleParams &sp,
+                                       const double *fr, S *state, S *buf2, S *buf3, long long o, bool fixed)
+{
+    EqState<double> q = eq_state<double>(rho, ux, uy, T, sp);
+    double f[NQ], h[NQ];
+    eq_all(q, f, h);
+    double sf = 0;
+    for (int i = 0; i < NQ; ++i) sf += f[i];
+    for (int i = 0; i < NQ; ++i) {
+        const long long of = sp.state_off + (long long)i * sp.plane + o;
+        const long long oh = sp.state_off + (long long)(NQ + i) * sp.plane + o;
+        const S fv = (S)(f[i] - fr[i]), hv = (S)(h[i] - fr[NQ + i]);
+        state[of] = fv;
+        state[oh] = hv;
+        if (fixed) {
+            buf2[of] = fv; buf3[of] = fv;
+            buf2[oh] = hv; buf3[oh] = hv;
+        }
+    }
+    return !(fabs(sf - rho) > 1e-6);
+}
+
 template <class S>
 __global__ void k_init(KArgs<S> a, const double *__restrict__ rho, const double *__restrict__ ux,
                        const double *__restrict__ uy, const double *__restrict__ T)
@@ -41,26 +67,11 @@ __global__ void k_init(KArgs<S> a, const double *__restrict__ rho, const double 
     const int x = t.x0 + threadIdx.x % a.tx, y = t.y0 + threadIdx.x / a.tx;
     if (x >= sp.nx || y >= sp.ny) return;
     const long long node = sp.node_off + (long long)y * sp.pitch + x;
-    EqState<double> q = eq_state<double>(rho[node], ux[node], uy[node], T[node], sp);
-    double f[NQ], h[NQ];
-    eq_all(q, f, h);
-    double sf = 0;
-    for (int i = 0; i < NQ; ++i) sf += f[i];
-    if (fabs(sf - rho[node]) > 1e-6) atomicOr(&a.status[t.sample], STATUS_EQ);
     const bool fixed = (a.nflags[node] & NF_TYPE) != 0;
     const long long o = (long long)y * sp.pitch + x;
-    const double *fr = a.fref + NPL * t.sample;
-    for (int i = 0; i < NQ; ++i) {
-        const S fv = (S)(f[i] - fr[i]), hv = (S)(h[i] - fr[NQ + i]);
-        plane_ptr(a.state, sp, i)[o] = fv;
-        plane_ptr(a.state, sp, NQ + i)[o] = hv;
-        if (fixed) {
-            plane_ptr(a.buf2, sp, i)[o] = fv;
-            plane_ptr(a.buf2, sp, NQ + i)[o] = hv;
-            plane_ptr(a.buf3, sp, i)[o] = fv;
-            plane_ptr(a.buf3, sp, NQ + i)[o] = hv;
-        }
-    }
+    if (!init_node<S>(rho[node], ux[node], uy[node], T[node], sp, a.fref + NPL * t.sample, a.state, a.buf2, a.buf3, o,
+                      fixed))
+        atomicOr(&a.status[t.sample], STATUS_EQ);
 }
 
 // ------------------------------------------------------------------ moments
@@ -834,22 +845,9 @@ __global__ void k_set_macro(const SampleParams *samples, int s, S *state, S *buf
     const long long n = (long long)sp.nx * sp.ny;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         const int y = (int)(k % sp.ny), x = (int)(k / sp.ny);
-        const EqState<double> q = eq_state<double>(fields[k], fields[n + k], fields[2 * n + k], fields[3 * n + k], sp);
-        double f[NQ], h[NQ];
-        eq_all(q, f, h);
         const long long o = (long long)y * sp.pitch + x;
         const bool fixed = (nflags[sp.node_off + o] & NF_TYPE) != 0;
-        for (int i = 0; i < NQ; ++i) {
-            const long long of = sp.state_off + (long long)i * sp.plane + o;
-            const long long oh = sp.state_off + (long long)(NQ + i) * sp.plane + o;
-            const S fv = (S)(f[i] - fr[i]), hv = (S)(h[i] - fr[NQ + i]);
-            state[of] = fv;
-            state[oh] = hv;
-            if (fixed) {
-                buf2[of] = fv; buf3[of] = fv;
-                buf2[oh] = hv; buf3[oh] = hv;
-            }
-        }
+        init_node<S>(fields[k], fields[n + k], fields[2 * n + k], fields[3 * n + k], sp, fr, state, buf2, buf3, o, fixed);
     }
 }
 
