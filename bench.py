@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--tile", default="0,0")
     ap.add_argument("--serving-seconds", type=float, default=45.0,
                     help="Poisson arrival window of the serving run (0: skip it)")
+    ap.add_argument("--no-probes", action="store_true",
+                    help="only the timed ensemble run: no accuracy, plain-FP64, serving or CPU runs (profiling)")
     return ap.parse_args()
 
 
@@ -472,21 +474,21 @@ def run_ours(args, rank, world, local_rank):
     e2e_value = nodes * world * args.steps / (e2e_ms * 1e3)
 
     extra = {}
-    if rank == 0:
+    if rank == 0 and not args.no_probes:
         extra["accuracy_vs_fp64"] = accuracy_probe(samples)
         try:
             extra["plain_fp64_mlups_32_samples"] = plain_fp64_probe(samples)
         except Exception as exc:  # reported, not fatal
             extra["plain_fp64_mlups_32_samples"] = "error: %s" % exc
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.no_probes:
         v, cores, kind, wall = cpu_reference_arm(os.cpu_count() or 1, 20, samples)
         cpu = {"value": v, "unit": "MLUPS", "cores": cores, "kind": kind,
                "sample": "%d processes, each one 64x64 ensemble sample x 20 steps (%.1f s wall)" % (cores, wall)}
 
     launches = b.launches_per_step(False) * args.steps
     b.close()
-    if rank == 0 and world == 1 and args.serving_seconds > 0:
+    if rank == 0 and world == 1 and args.serving_seconds > 0 and not args.no_probes:
         try:
             extra["serving"] = serving_probe(args.serving_seconds, value)
         except Exception as exc:  # reported, not fatal
