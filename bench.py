@@ -228,6 +228,27 @@ def plain_fp64_probe(samples, steps=10, n=32):
     return lu / wall / 1e6
 
 
+def rank_seed(seed, rank):
+    """Each rank advances its own seeded ensemble; rank 0 is the 1-GPU run."""
+    return seed + 7919 * rank
+
+
+def reduce_over_ranks(x, dist, op, device):
+    """x reduced over the ranks (dist None: one rank); op 'sum' or 'max'."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM if op == "sum" else dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_mlups(total_nodes, steps, max_ms):
+    """Whole-job MLUPS: all ranks' lattice updates over the slowest rank's time."""
+    return total_nodes * steps / (max_ms * 1e3)
+
+
 SERVE_SIDES = (32, 1024)      # square grid side ~ U{32..1024}
 SERVE_STEPS = (200, 5000)     # step count ~ U{200..5000}
 
@@ -388,7 +409,7 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
 
-    samples = W.uq_ensemble(n=args.samples, seed=args.seed + 7919 * rank)
+    samples = W.uq_ensemble(n=args.samples, seed=rank_seed(args.seed, rank))
     cases = [W.ensemble_case(d) for d in samples]
     tx, ty = (int(v) for v in args.tile.split(","))
     b = Batch(cases, precision=args.precision, tile=(tx, ty))
@@ -400,11 +421,9 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_over_ranks(x, dist, "max", "cuda")
+
+    total_nodes = reduce_over_ranks(nodes, dist, "sum", "cuda")
 
     b.step(args.warmup)
     torch.cuda.synchronize()
@@ -423,7 +442,7 @@ def run_ours(args, rank, world, local_rank):
     ms = max_over_ranks(e0.elapsed_time(e1))
     ms_per_step = ms / args.steps
     status = b.status()
-    value = nodes * world * args.steps / (ms * 1e3)
+    value = aggregate_mlups(total_nodes, args.steps, ms)
 
     # per-phase device time (CUDA events on the batch's stream, no graph)
     phases = b.profile(3)
@@ -471,7 +490,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     barrier()
     e2e_ms = max_over_ranks(e2.elapsed_time(e3))
-    e2e_value = nodes * world * args.steps / (e2e_ms * 1e3)
+    e2e_value = aggregate_mlups(total_nodes, args.steps, e2e_ms)
 
     extra = {}
     if rank == 0 and not args.no_probes:
@@ -501,7 +520,8 @@ def run_ours(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "f32" else "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "samples_per_gpu": n_s, "sides": [64, 128, 256, 512],
-                       "nodes_per_step_per_gpu": nodes, "steps_per_solve": 1000,
+                       "nodes_per_step_per_gpu": nodes, "nodes_per_step_total": int(total_nodes),
+                       "steps_per_solve": 1000,
                        "precision": "FP32 state/stencils/collision, FP64 moment sums" if args.precision == "f32"
                        else "FP64", "l2": "inputs larger than L2 (whole-ensemble state ~%.1f GB)" %
                        (nodes * 26 * 4 * (4 if args.precision == "f32" else 8) / 1e9),

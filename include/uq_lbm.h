@@ -267,6 +267,16 @@ LBM_API lbm_status lbm_server_get_stats(lbm_server *s, lbm_server_stats *st);
 /* Stop the threads; solves not done are dropped. */
 LBM_API void lbm_server_destroy(lbm_server *s);
 
+/* ------------------------------------------------------------ self-test
+ * No counterpart in the reference.  Exercises the bounded wait that every
+ * device-side wait of the stencil kernels uses (an mbarrier polled a fixed
+ * number of times): one block waits on a barrier that expects one arrival.
+ * arrive = 0: nothing arrives, the wait gives up, the block records the
+ * timeout bit and exits, and the call returns LBM_ERR_TIMEOUT with the
+ * device still usable.  arrive = 1: the arrival comes first and the call
+ * returns LBM_OK.  Nothing traps or faults either way. */
+LBM_API lbm_status lbm_selftest_bounded_wait(int arrive);
+
 /* ------------------------------------------------- allocation-free step
  * No counterpart in the reference.  For callers that cannot call
  * cudaMalloc: an application that owns all device memory through its own

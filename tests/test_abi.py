@@ -59,3 +59,19 @@ def test_invalid_config_is_rejected():
     h = ctypes.c_void_p()
     assert L.lbm_create(ctypes.byref(cfg), ctypes.byref(ini), 0, ctypes.byref(h)) == native.LBM_ERR_INVALID
     assert not h.value
+
+
+def test_server_and_selftest_without_gpu_fail_loudly():
+    import torch
+
+    if torch.cuda.is_available():
+        return
+    from uq_b200.solver import Server
+
+    try:
+        Server(precision="f32")
+    except native.LbmError as e:
+        assert e.code == native.LBM_ERR_CUDA
+    else:
+        raise AssertionError("lbm_server_create succeeded without a CUDA device")
+    assert native.lib().lbm_selftest_bounded_wait(0) == native.LBM_ERR_CUDA

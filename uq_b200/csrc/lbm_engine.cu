@@ -957,6 +957,24 @@ void *lbm_batch_stream(lbm_batch *b) { return b ? (void *)b->stream : nullptr; }
 
 long long lbm_batch_nodes(lbm_batch *b) { return b ? b->lattice_nodes : 0; }
 
+lbm_status lbm_selftest_bounded_wait(int arrive)
+{
+    API_BEGIN
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
+        throw LbmError(LBM_ERR_CUDA, "no CUDA device available (this library has no CPU path)");
+    DevBuf<int> st;
+    st.alloc(1);
+    CU(cudaMemset(st.p, 0, sizeof(int)));
+    CU(launch_wait_selftest(st.p, arrive ? 1 : 0, nullptr));
+    int bits = 0;
+    CU(cudaMemcpy(&bits, st.p, sizeof(int), cudaMemcpyDeviceToHost));
+    const lbm_status r = lbm_batch::to_status(bits);
+    if (r != LBM_OK) g_last_error = "bounded device wait ran out";
+    return r;
+    API_END
+}
+
 lbm_status lbm_batch_step(lbm_batch *b, int n_steps, int want_residual)
 {
     API_BEGIN

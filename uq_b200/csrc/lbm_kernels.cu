@@ -936,6 +936,31 @@ cudaError_t launch_dist_io(const SampleParams *samples, int s, S *state, S *buf2
     return cudaGetLastError();
 }
 
+// Self-test of the bounded mbarrier wait the stencil kernels use: one block
+// initialises a barrier that expects one arrival and waits on it with the
+// same poll limit.  With arrive = 0 nothing arrives, the wait runs out and
+// the block records STATUS_TIMEOUT and returns; with arrive = 1 thread 0
+// arrives first and the wait succeeds.  No copy is ever in flight.
+__global__ void k_wait_selftest(int *status, int arrive, uint32_t polls)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && arrive) mbar_arrive_expect_tx(&bar, 0);
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0, polls);
+    if (!ok && threadIdx.x == 0) atomicOr(status, STATUS_TIMEOUT);
+}
+
+cudaError_t launch_wait_selftest(int *status, int arrive, cudaStream_t st)
+{
+    k_wait_selftest<<<1, 32, 0, st>>>(status, arrive, TMA_WAIT_POLLS);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_residual(const SampleParams *samples, int nsamples, const double *partial, const int *tile_first,
                             const int *tile_count, double *residual, cudaStream_t st)
 {

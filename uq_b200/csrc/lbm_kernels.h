@@ -65,6 +65,7 @@ cudaError_t launch_dist_io(const SampleParams *samples, int s, S *state, S *buf2
 template <class S>
 cudaError_t launch_set_macro(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, const double *fields,
                              const uint8_t *nflags, const double *fref, long long nodes, cudaStream_t st);
+cudaError_t launch_wait_selftest(int *status, int arrive, cudaStream_t st);
 cudaError_t launch_residual(const SampleParams *samples, int nsamples, const double *partial, const int *tile_first,
                             const int *tile_count, double *residual, cudaStream_t st);
 

@@ -123,6 +123,7 @@ SIGNATURES = {
     "lbm_server_release": (C.c_int, [C.c_void_p, C.c_longlong]),
     "lbm_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(LbmServerStats)]),
     "lbm_server_destroy": (None, [C.c_void_p]),
+    "lbm_selftest_bounded_wait": (C.c_int, [C.c_int]),
     "lbm_step_noalloc": (C.c_int, [C.POINTER(LbmConfig), C.c_int, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_int,
                                    C.c_void_p]),
 }
