@@ -415,12 +415,26 @@ __device__ __forceinline__ C minmod(C a, C b)
     return a * b > C(0) ? (fabs(a) < fabs(b) ? a : b) : C(0);
 }
 
+// Round-to-nearest operations the compiler may neither fuse nor split:
+// NND and WENO5 are written with them so that every compiled instance (the
+// simple-tile paths per scheme, the boundary-aware paths, the wall factors)
+// rounds a face flux the same way, and results do not depend on which path
+// a node took (tile shape, batch packing).
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // NND (cpuLBM.cpp:1328-1356) on the 3 upwind-ordered values s0, s1, s2
 template <class C>
 __device__ __forceinline__ C nnd3(C ae, C s0, C s1, C s2)
 {
-    const C c = ae * s1;
-    return c + C(0.5) * minmod<C>(ae * s2 - c, c - ae * s0);
+    const C c = xmul(ae, s1);
+    return xfma(C(0.5), minmod<C>(xfma(ae, s2, -c), xfma(-ae, s0, c)), c);
 }
 
 // one division per face (the FP64 path keeps it correctly rounded)
@@ -434,18 +448,25 @@ __device__ __forceinline__ float face_div(float n, float d) { return __fdividef(
 template <class C>
 __device__ __forceinline__ C weno5(C ae, C s0, C s1, C s2, C s3, C s4)
 {
-    const C q0 = ae * s0, q1 = ae * s1, q2 = ae * s2, q3 = ae * s3, q4 = ae * s4;
-    const C d0 = q0 - C(2) * q1 + q2, d1 = q1 - C(2) * q2 + q3, d2 = q2 - C(2) * q3 + q4;
-    const C l0 = q0 - C(4) * q1 + C(3) * q2, l1 = q1 - q3, l2 = C(3) * q2 - C(4) * q3 + q4;
-    const C a0 = C(1e-6) + (C(13.0 / 12.0) * d0 * d0 + C(0.25) * l0 * l0);
-    const C a1 = C(1e-6) + (C(13.0 / 12.0) * d1 * d1 + C(0.25) * l1 * l1);
-    const C a2 = C(1e-6) + (C(13.0 / 12.0) * d2 * d2 + C(0.25) * l2 * l2);
-    const C p0 = a0 * a0, p1 = a1 * a1, p2 = a2 * a2;
-    const C w0 = C(0.1) * (p1 * p2), w1 = C(0.6) * (p0 * p2), w2 = C(0.3) * (p0 * p1);
-    const C r0 = (C(2) * q0 - C(7) * q1 + C(11) * q2);
-    const C r1 = (-q1 + C(5) * q2 + C(2) * q3);
-    const C r2 = (C(2) * q2 + C(5) * q3 - q4);
-    return face_div(w0 * r0 + w1 * r1 + w2 * r2, C(6) * (w0 + w1 + w2));
+    const C q0 = xmul(ae, s0), q1 = xmul(ae, s1), q2 = xmul(ae, s2), q3 = xmul(ae, s3), q4 = xmul(ae, s4);
+    // second differences d_k and one-sided slopes l_k of the three stencils
+    const C d0 = xfma(C(-2), q1, xadd(q0, q2));
+    const C d1 = xfma(C(-2), q2, xadd(q1, q3));
+    const C d2 = xfma(C(-2), q3, xadd(q2, q4));
+    const C l0 = xfma(C(3), q2, xfma(C(-4), q1, q0));
+    const C l1 = xsub(q1, q3);
+    const C l2 = xfma(C(-4), q3, xfma(C(3), q2, q4));
+    // eps + b_k
+    const C a0 = xfma(xmul(C(13.0 / 12.0), d0), d0, xfma(xmul(C(0.25), l0), l0, C(1e-6)));
+    const C a1 = xfma(xmul(C(13.0 / 12.0), d1), d1, xfma(xmul(C(0.25), l1), l1, C(1e-6)));
+    const C a2 = xfma(xmul(C(13.0 / 12.0), d2), d2, xfma(xmul(C(0.25), l2), l2, C(1e-6)));
+    const C p0 = xmul(a0, a0), p1 = xmul(a1, a1), p2 = xmul(a2, a2);
+    const C w0 = xmul(C(0.1), xmul(p1, p2)), w1 = xmul(C(0.6), xmul(p0, p2)), w2 = xmul(C(0.3), xmul(p0, p1));
+    // candidate reconstructions (times 6)
+    const C r0 = xfma(C(11), q2, xfma(C(-7), q1, xmul(C(2), q0)));
+    const C r1 = xfma(C(2), q3, xfma(C(5), q2, -q1));
+    const C r2 = xsub(xfma(C(5), q3, xmul(C(2), q2)), q4);
+    return face_div(xfma(w2, r2, xfma(w1, r1, xmul(w0, r0))), xmul(C(6), xadd(xadd(w0, w1), w2)));
 }
 
 // view of one sample's stage buffer and node flags

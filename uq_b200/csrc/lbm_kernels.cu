@@ -193,23 +193,26 @@ __device__ __forceinline__ C line_flux(const SampleParams &sp, const S *__restri
 // Stage tiles in shared memory: per direction the f and h planes over the
 // box [x0-4, x0+TX+4) x [y0-3, y0+TY+3) (x start kept on a 16-byte
 // boundary), loaded by TMA ahead of use.  Directions are processed in
-// groups of G (G = 2 pairs each direction with its opposite, halving the
-// barriers; G = 1 on the FP64 path, whose boxes are twice as large).
+// groups of G, one barrier per group: G = 4 on the FP32 path (two +/-
+// pairs per group: 3 barriers per phase, and the tile-edge items of four
+// directions spread over more warps); G = 1 on the FP64 path, whose boxes
+// are twice as large.
 constexpr int HALO_X = 4, HALO_Y = 3;
 constexpr uint32_t TMA_WAIT_POLLS = 1u << 16;
 
 template <int G>
 struct GroupCfg {
-    static constexpr int NSTAGE = G == 2 ? 2 : 3;  // groups in flight
+    static constexpr int NSTAGE = G >= 2 ? 2 : 3;  // groups in flight
     static constexpr int NGROUP = 12 / G;
 };
 
 // direction m of group g: G = 1 -> 1..12; G = 2 -> (1,3) (2,4) (5,7) (6,8)
-// (9,11) (10,12)
+// (9,11) (10,12); G = 4 -> (1,3,2,4) (5,7,6,8) (9,11,10,12)
 template <int G>
 __host__ __device__ __forceinline__ int group_dir(int g, int m)
 {
     if (G == 1) return g + 1;
+    if (G == 4) return 4 * g + 1 + (m >> 1) + 2 * (m & 1);
     const int base = g < 2 ? g + 1 : (g < 4 ? g + 3 : g + 5);
     return base + 2 * m;
 }
@@ -274,10 +277,11 @@ __device__ __forceinline__ void issue_group_load(TileCtx<S, C> &k, int g, int sl
 
 // reconstruction from the staged box (fast path; no solid, no domain edge
 // within the stencil): element step `st` in the box, upwind sign folded in
-template <class S, class C>
+// FM: 1 WENO5, 0 NND, -1 the sample's FMETHOD (read at run time)
+template <class S, class C, int FM = -1>
 __device__ __forceinline__ C box_flux(const SampleParams &sp, const S *c0, int st, C ae)
 {
-    if (sp.fm) return weno5<C>(ae, (C)c0[-2 * st], (C)c0[-st], (C)c0[0], (C)c0[st], (C)c0[2 * st]);
+    if (FM == 1 || (FM < 0 && sp.fm)) return weno5<C>(ae, (C)c0[-2 * st], (C)c0[-st], (C)c0[0], (C)c0[st], (C)c0[2 * st]);
     return nnd3<C>(ae, (C)c0[-st], (C)c0[0], (C)c0[st]);
 }
 
@@ -315,7 +319,7 @@ __device__ __forceinline__ C any_node_flux(TileCtx<S, C> &k, const S *box, int i
 // Own-node face fluxes of direction i into sf_m (fx_f, fx_h, fy_f, fy_h)
 // and the upwind fluxes across the tile edges into ringx_m / ringy_m
 // (items numbered from ring0 over the block's threads).
-template <class S, class C, bool SIMPLE>
+template <class S, class C, bool SIMPLE, int FM>
 __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const S *box, C *sf, C *ringx, C *ringy,
                                            int ring0)
 {
@@ -336,22 +340,22 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
         const S *cf = box + ly * k.BW + lx;
         const S *ch = cf + k.pstride;
         if (SX) {
-            sf[k.tid] = box_flux<S, C>(sp, cf, SX, aex);
-            sf[NT + k.tid] = box_flux<S, C>(sp, ch, SX, aex);
+            sf[k.tid] = box_flux<S, C, FM>(sp, cf, SX, aex);
+            sf[NT + k.tid] = box_flux<S, C, FM>(sp, ch, SX, aex);
         }
         if (SY) {
-            sf[2 * NT + k.tid] = box_flux<S, C>(sp, cf, SY * k.BW, aey);
-            sf[3 * NT + k.tid] = box_flux<S, C>(sp, ch, SY * k.BW, aey);
+            sf[2 * NT + k.tid] = box_flux<S, C, FM>(sp, cf, SY * k.BW, aey);
+            sf[3 * NT + k.tid] = box_flux<S, C, FM>(sp, ch, SY * k.BW, aey);
         }
         for (int r = r0; r < nx_items + ny_items; r += NT) {
             if (r < nx_items) {
                 const int fh = r / k.TY, row = r % k.TY;
                 const int bx = (SX > 0 ? -1 : k.TX) + HALO_X, by = row + HALO_Y;
-                ringx[fh * k.TY + row] = box_flux<S, C>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SX, aex);
+                ringx[fh * k.TY + row] = box_flux<S, C, FM>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SX, aex);
             } else {
                 const int q = r - nx_items, fh = q / k.TX, col = q % k.TX;
                 const int bx = col + HALO_X, by = (SY > 0 ? -1 : k.TY) + HALO_Y;
-                ringy[fh * k.TX + col] = box_flux<S, C>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SY * k.BW, aey);
+                ringy[fh * k.TX + col] = box_flux<S, C, FM>(sp, box + (size_t)fh * k.pstride + by * k.BW + bx, SY * k.BW, aey);
             }
         }
         return;
@@ -469,7 +473,7 @@ __device__ __forceinline__ void dir_divergence(TileCtx<S, C> &k, const int i, co
 // (posFluxes/computeFlux, cpuLBM.cpp:1405-1500; solid nodes answer
 // wallFluxes' alpha |e| f, cpuLBM.cpp:1576-1586) and edge fluxes of each,
 // one barrier, refill the slot, then each direction's divergence.
-template <class S, class C, bool SIMPLE, int G>
+template <class S, class C, bool SIMPLE, int G, int FM>
 __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
 {
     constexpr int NST = GroupCfg<G>::NSTAGE;
@@ -491,7 +495,7 @@ __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
         C *sf = k.sf + (size_t)(buf * G + m) * 4 * NT;
         C *rx = k.ringx + (size_t)(buf * G + m) * 2 * k.TY;
         C *ry = k.ringy + (size_t)(buf * G + m) * 2 * k.TX;
-        dir_fluxes<S, C, SIMPLE>(k, i, boxes + (size_t)(2 * m) * k.pstride, sf, rx, ry, ring0);
+        dir_fluxes<S, C, SIMPLE, FM>(k, i, boxes + (size_t)(2 * m) * k.pstride, sf, rx, ry, ring0);
         ring0 += (c_EX[i] ? 2 * k.TY : 0) + (c_EY[i] ? 2 * k.TX : 0);
         while (ring0 >= NT) ring0 -= NT;
     }
@@ -513,13 +517,13 @@ __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
 
 template <class S>
 struct FluxGroup {
-    static constexpr int value = sizeof(S) == 4 ? 2 : 1;
+    static constexpr int value = sizeof(S) == 4 ? 4 : 1;
 };
 
 size_t flux_smem_bytes_t(size_t es, int tx, int ty)
 {
-    const int G = es == 4 ? 2 : 1;
-    return flux_layout(es, es, tx, ty, G, G == 2 ? GroupCfg<2>::NSTAGE : GroupCfg<1>::NSTAGE).total;
+    const int G = es == 4 ? 4 : 1;
+    return flux_layout(es, es, tx, ty, G, G == 4 ? GroupCfg<4>::NSTAGE : GroupCfg<1>::NSTAGE).total;
 }
 
 // MODE: 1 = RK3 stage 3 (fluxes of buffer 2), 2 = RK3 final (buffer 3),
@@ -590,11 +594,17 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     sD[tid] = C(0);          // direction 0 streams nothing
     sD[NQ * NT + tid] = C(0);
     if (tile_simple(t)) {
+        // simple tiles: the flux scheme fixed at compile time (smaller hot code)
+        if (sp.fm) {
 #pragma unroll 1
-        for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G>(k, g);
+            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 1>(k, g);
+        } else {
+#pragma unroll 1
+            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 0>(k, g);
+        }
     } else {
 #pragma unroll 1
-        for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, false, G>(k, g);
+        for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, false, G, -1>(k, g);
     }
 
     double res_part = 0;
@@ -604,6 +614,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
         S *__restrict__ b3 = a.buf3 + sp.state_off;
         const C dt = (C)sp.dt;
         bool final_phase = true;
+        double fin_r = 0, fin_sh = 0;  // FP64 sums of the new state (MODE 2)
         if (MODE == 1) {
             // RK3 stage 3 (cpuLBM.cpp:1928-1993) and the part of the update
             // (cpuLBM.cpp:1999-2042) that does not need the stage-3 fluxes
@@ -682,14 +693,24 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             if (fabs(sf3 - (rho3 - sp.rho0)) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(rho3))))
                 atomicOr(&a.status[t.sample], STATUS_EQ);
         } else if (MODE == 2) {
-            // final RK3 combination (cpuLBM.cpp:1999-2042): f = acc - D3/2;
-            // all loads first, then the stores (no load waits behind a store)
-            S acc[NPL];
+            // final RK3 combination (cpuLBM.cpp:1999-2042): f = acc - D3/2,
+            // f planes then h planes (loads of a half before its stores),
+            // summing the new values in FP64 for the finiteness check
 #pragma unroll
-            for (int p = 0; p < NPL; ++p) acc[p] = st[(long long)p * sp.plane + o];
+            for (int half = 0; half < 2; ++half) {
+                S acc[NQ];
 #pragma unroll
-            for (int p = 0; p < NPL; ++p)
-                st[(long long)p * sp.plane + o] = (S)((C)acc[p] - C(0.5) * sD[p * NT + tid]);
+                for (int i = 0; i < NQ; ++i) acc[i] = st[(long long)(half * NQ + i) * sp.plane + o];
+                double sum = 0;
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) {
+                    const S v = (S)((C)acc[i] - C(0.5) * sD[(half * NQ + i) * NT + tid]);
+                    st[(long long)(half * NQ + i) * sp.plane + o] = v;
+                    sum += (double)v;
+                }
+                if (half == 0) fin_r = sum;
+                else fin_sh = sum;
+            }
         } else {
             // RK1 update (cpuLBM.cpp:1674-1710), EULER (:2130-2168), EULER_EQ (:2220-2258)
             const Macro m = node_macro(st, sp, o);
@@ -750,11 +771,13 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                 res_part = d * d;
             } else {
                 // finiteness / positive density from the FP64 sums alone
-                double r = 0, sh = 0;
+                double r = fin_r, sh = fin_sh;
+                if (MODE != 2) {
 #pragma unroll
-                for (int i = 0; i < NQ; ++i) {
-                    r += (double)st[(long long)i * sp.plane + o];
-                    sh += (double)st[(long long)(NQ + i) * sp.plane + o];
+                    for (int i = 0; i < NQ; ++i) {
+                        r += (double)st[(long long)i * sp.plane + o];
+                        sh += (double)st[(long long)(NQ + i) * sp.plane + o];
+                    }
                 }
                 r += sp.rho0;
                 if (!(r > 0.0) || !isfinite(r) || !isfinite(sh)) atomicOr(&a.status[t.sample], STATUS_NONFINITE);
