@@ -180,28 +180,108 @@ def run_reference_impl(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def field_errors(m, r):
+    """Relative L2 and max-norm differences of rho, |u| (vector difference)
+    and T between two macro dicts (m against the reference r)."""
+    out = {}
+    for name in ("rho", "u", "T"):
+        if name == "u":
+            d = np.sqrt((m["ux"] - r["ux"]) ** 2 + (m["uy"] - r["uy"]) ** 2)
+            ref = np.hypot(r["ux"], r["uy"])
+        else:
+            d = np.abs(m[name] - r[name])
+            ref = np.abs(r[name])
+        out[name] = (float(np.linalg.norm(d) / max(np.linalg.norm(ref), 1e-300)),
+                     float(d.max() / max(ref.max(), 1e-300)))
+    return out
+
+
 def accuracy_probe(samples, steps=10):
-    """Mixed path vs the FP64 plain path on a few small samples after
-    `steps` steps: max relative L2 of rho, |u|, T."""
+    """Mixed path vs the FP64 path on every sample of the ensemble after
+    `steps` steps: per-sample relative L2 of rho, |u|, T; the worst sample,
+    the median and the count within 1e-5."""
     from uq_b200 import workloads as W
     from uq_b200.solver import Batch
 
-    small = [d for d in samples if d["nx"] <= 128][:8]
-    cases = [W.ensemble_case(d) for d in small]
+    cases = [W.ensemble_case(d) for d in samples]
     b32 = Batch(cases, "f32")
     b64 = Batch(cases, "f64")
     b32.step(steps)
     b64.step(steps)
-    worst = {"rho": 0.0, "u": 0.0, "T": 0.0}
+    per = {"rho": [], "u": [], "T": []}
     for k in range(len(cases)):
-        m, r = b32.macro(k), b64.macro(k)
-        worst["rho"] = max(worst["rho"], np.linalg.norm(m["rho"] - r["rho"]) / np.linalg.norm(r["rho"]))
-        worst["T"] = max(worst["T"], np.linalg.norm(m["T"] - r["T"]) / np.linalg.norm(r["T"]))
-        du = np.sqrt((m["ux"] - r["ux"]) ** 2 + (m["uy"] - r["uy"]) ** 2)
-        worst["u"] = max(worst["u"], np.linalg.norm(du) / np.linalg.norm(np.hypot(r["ux"], r["uy"])))
+        e = field_errors(b32.macro(k), b64.macro(k))
+        for name in per:
+            per[name].append(e[name][0])
     b32.close()
     b64.close()
-    return {"steps": steps, "samples": len(cases), "l2_rel_max": worst}
+    worst = {k: float(np.max(v)) for k, v in per.items()}
+    med = {k: float(np.median(v)) for k, v in per.items()}
+    ok = int(sum(all(per[k][j] <= 1e-5 for k in per) for j in range(len(cases))))
+    return {"steps": steps, "samples": len(cases), "l2_rel_max": worst, "l2_rel_median": med,
+            "samples_within_1e-5": ok}
+
+
+def config_probes(seed=99):
+    """The other full-size workloads, bounded.
+
+    Riemann 2048 x 2048 (Lax-Liu 3, NND, RK1 -- the reference has no RK2 --,
+    tau 1e-3, 500 steps): FP32 and FP64 timed on the device, then the FP32
+    fields against the FP64 ones.  Flat plate, 16 samples of 2048 x 512 on
+    the y-stretched grid with Ma ~ U(1.5, 2.5), tau ~ U(5e-4, 2e-3) (WENO5,
+    RK3): FP32 timed over 50 steps (of the configuration's 20000), and FP32
+    against FP64 after 10 steps."""
+    import torch
+
+    from uq_b200 import workloads as W
+    from uq_b200.solver import Batch
+
+    def timed(b, n):
+        st = torch.cuda.ExternalStream(b.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        b.step(n)
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    out = {}
+    case = W.riemann(nx=2048, ny=2048, steps=500)
+    res = {}
+    for prec in ("f32", "f64"):
+        b = Batch([case], prec)
+        ms = timed(b, 500)
+        res[prec] = (b.nodes * 500 / (ms * 1e3), int(b.status()[0]), b.macro(0))
+        b.close()
+    err = field_errors(res["f32"][2], res["f64"][2])
+    out["riemann_2048_nnd_rk1_500"] = {
+        "mlups_f32": res["f32"][0], "mlups_f64": res["f64"][0], "status_f32": res["f32"][1],
+        "status_f64": res["f64"][1], "f32_vs_f64_l2": {k: v[0] for k, v in err.items()},
+        "f32_vs_f64_linf": {k: v[1] for k, v in err.items()}}
+    rng = np.random.default_rng(seed)
+    draws = [(float(rng.uniform(1.5, 2.5)), float(rng.uniform(5e-4, 2e-3))) for _ in range(16)]
+    plates = [W.flat_plate(mach=m, tau=t, steps=20000) for m, t in draws]
+    b = Batch(plates, "f32")
+    b.step(2)
+    ms = timed(b, 50)
+    mlups = b.nodes * 50 / (ms * 1e3)
+    st50 = b.status()
+    b.close()
+    b32, b64 = Batch(plates, "f32"), Batch(plates, "f64")
+    b32.step(10)
+    b64.step(10)
+    worst = {"rho": 0.0, "u": 0.0, "T": 0.0}
+    for k in range(len(plates)):
+        e = field_errors(b32.macro(k), b64.macro(k))
+        for name in worst:
+            worst[name] = max(worst[name], e[name][0])
+    b32.close()
+    b64.close()
+    out["flat_plate_16x2048x512_weno5_rk3"] = {
+        "mlups_f32": mlups, "steps_timed": 50, "status_ok_after_52_steps": int((st50 == 0).sum()),
+        "f32_vs_f64_l2_max_10_steps": worst}
+    return out
 
 
 def plain_fp64_probe(samples, steps=10, n=32):
@@ -495,6 +575,10 @@ def run_ours(args, rank, world, local_rank):
     extra = {}
     if rank == 0 and not args.no_probes:
         extra["accuracy_vs_fp64"] = accuracy_probe(samples)
+        try:
+            extra["configs"] = config_probes()
+        except Exception as exc:  # reported, not fatal
+            extra["configs"] = {"error": repr(exc)}
         try:
             extra["plain_fp64_mlups_32_samples"] = plain_fp64_probe(samples)
         except Exception as exc:  # reported, not fatal

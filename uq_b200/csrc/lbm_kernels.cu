@@ -91,9 +91,15 @@ __device__ __forceinline__ Macro node_macro(const S *__restrict__ st, const Samp
 }
 
 // ------------------------------------------------------------------- P0
-// RK: 1 (RK3 stages 1+2), 0 (RK1 stage 1), 2 (EULER / EULER_EQ: copy)
+// RK: 1 (RK3 stages 1+2), 0 (RK1 stage 1), 2 (EULER / EULER_EQ: copy).
+// Pointwise and memory-bound: the FP32 instances keep 64 registers so that
+// four blocks (32 warps) per SM keep loads in flight.
+template <class S>
+struct Stage0Blocks {
+    static constexpr int value = sizeof(S) == 4 ? 4 : 2;
+};
 template <class S, class C, int RK>
-__global__ void __launch_bounds__(256, 2) k_stage0(KArgs<S> a)
+__global__ void __launch_bounds__(256, Stage0Blocks<S>::value) k_stage0(KArgs<S> a)
 {
     const Tile t = a.tiles[blockIdx.x];
     const SampleParams sp = a.samples[t.sample];
