@@ -136,6 +136,32 @@ LBM_API void lbm_destroy(lbm_handle *h);
 /* Human-readable message of the last failure on the calling thread. */
 LBM_API const char *lbm_last_error(void);
 
+/* ------------------------------------------------------------- MAT files
+ * The reference's MATLAB Level-5 files at the boundary.  Input: the
+ * variables cpuLBM::loadInput reads (cpuLBM.cpp:46-281), same names, any
+ * numeric class (converted to double as loadInput's mxGetPr reads it),
+ * compressed or not; bndArray's y axis is flipped as loadInput does.
+ * Output: the variables cpuLBM::createMAT writes (cpuLBM.cpp:467-745). */
+typedef struct lbm_mat_case lbm_mat_case;
+
+/* Read an input MAT file into a case (no GPU needed). */
+LBM_API lbm_status lbm_mat_read_case(const char *path, lbm_mat_case **out);
+/* The case as the lbm_create arguments; init's arrays stay owned by the
+ * case (valid until lbm_mat_case_free).  Either pointer may be NULL. */
+LBM_API lbm_status lbm_mat_case_get(const lbm_mat_case *c, lbm_config *cfg, lbm_init *init);
+LBM_API void lbm_mat_case_free(lbm_mat_case *c);
+/* new cpuLBM(files) on an input MAT file: read it and create a handle. */
+LBM_API lbm_status lbm_create_from_mat(const char *path, int precision, lbm_handle **out);
+/* createMAT: rho, ux, uy, p, T as {Ny, Nx} arrays over [x*Ny + y], t, dx,
+ * dy and, when f, h, ex, ey are all given, f and h as {13, Ny, Nx} over
+ * [(x*Ny + y)*13 + i] with the lattice vectors ex, ey (no GPU needed). */
+LBM_API lbm_status lbm_mat_write_fields(const char *path, int Nx, int Ny, const double *rho, const double *ux,
+                                        const double *uy, const double *p, const double *T, double t, double dx,
+                                        double dy, const double *f, const double *h, const double *ex,
+                                        const double *ey);
+/* createMAT(name, DF) of a handle's current state (t = step * dt). */
+LBM_API lbm_status lbm_write_mat(lbm_handle *h, const char *path, int with_dist);
+
 /* -------------------------------------------------------------- batches
  * Many independent samples (uneven grids, own parameters) advanced
  * together: every phase is one launch over a packed tile list of all

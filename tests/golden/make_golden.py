@@ -8,6 +8,7 @@ Each fixture records the case builder and its arguments
 checksum of that input to catch builder drift.
 
     python tests/golden/make_golden.py          # regenerate all fixtures
+    python tests/golden/make_golden.py mat      # only the MAT-input fixture
 
 Needs the reference tree (only in the development container); the fixtures
 themselves are committed and need nothing at test time.
@@ -57,9 +58,43 @@ def save(name, entries):
     print(name, len(entries), "cases")
 
 
+MAT_INPUT = "/root/reference/Items/11.04.06-BoundaryLayer-Jacobs/input.mat"
+
+
+def mat_input():
+    """The reference's own input file (a Mach-2 boundary layer, 1001 x 101,
+    R = 287, Tc_Tref = 2.5) read by the library's MAT reader and by scipy
+    (they must agree), then 2 steps of the reference binary on it."""
+    import scipy.io as sio
+
+    from uq_b200.solver import mat_case
+
+    case = mat_case(MAT_INPUT)
+    raw = sio.loadmat(MAT_INPUT)
+    for k, v in raw.items():
+        if k.startswith("__") or k in ("bndArray",) or k not in case:
+            continue
+        assert np.allclose(np.ravel(case[k])[: np.size(v)], np.ravel(v).astype(np.float64)), k
+    bnd = np.asarray(raw["bndArray"], dtype=np.int64)  # (Ny, Nx), y flipped by loadInput
+    assert np.array_equal(case["bnd"], bnd[::-1, :].T)
+    # nPrintOut / MAT are driver output switches, not part of the case
+    r = refrun.run_reference(dict(case, nPrintOut=1 << 30, MAT=0), max_steps=2)
+    arrays = {"case_" + k: np.asarray(v) for k, v in case.items() if k != "bnd"}
+    arrays["case_bnd"] = case["bnd"].astype(np.uint8)
+    for k in ("rho", "ux", "uy", "T"):
+        arrays["out_" + k] = r[k]
+    arrays["out_step"] = np.asarray(r["step"])
+    arrays["out_dt"] = np.asarray(r["dt"])
+    np.savez_compressed(os.path.join(OUT, "mat_boundary_layer.npz"), **arrays)
+    print("mat_boundary_layer.npz", case["bnd"].shape, "steps", r["step"])
+
+
 def main():
     if not refrun.available():
         sys.exit("reference binary missing: make -C oracle")
+    if sys.argv[1:] == ["mat"]:
+        mat_input()
+        return
 
     # (i) two steps from seeded random states: every BC family x flux x stepper
     entries = []
@@ -103,6 +138,8 @@ def main():
     # (ii) the full Couette workload: 64x128, WENO5, RK3, 2000 steps
     save("couette_64x128_2000.npz",
          [run("couette", dict(nx=64, ny=128, steps=2000, seed=0), keep=("rho", "ux", "uy", "T"))])
+
+    mat_input()
 
 
 if __name__ == "__main__":

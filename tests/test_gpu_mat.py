@@ -1,0 +1,69 @@
+"""A solve created from an input MAT file and written back to one.
+
+The case is the reference's own boundary-layer input (a committed fixture
+made from its input.mat), written to a MAT file the way that file stores
+its variables (integer classes, compressed).  Created from that file, the
+FP64 path must reproduce the reference solver's two steps on it; the FP32
+path must stay within the mixed-precision tolerance; the MAT output must
+hold the handle's fields and distributions in createMAT's layout.
+"""
+import numpy as np
+import pytest
+
+from uq_b200.solver import Solver
+
+from golden_util import rel_l2, rel_max
+from test_mat_io import _as_mat_vars, _fixture_case
+
+pytestmark = pytest.mark.gpu
+sio = pytest.importorskip("scipy.io")
+
+
+@pytest.fixture(scope="module")
+def mat_input(tmp_path_factory):
+    case, ref = _fixture_case()
+    p = tmp_path_factory.mktemp("mat") / "input.mat"
+    sio.savemat(str(p), _as_mat_vars(case, integer_classes=True), do_compression=True)
+    return p, case, ref
+
+
+def test_fp64_from_mat_matches_reference(cuda_device, mat_input):
+    p, case, ref = mat_input
+    s = Solver.from_mat(p, "f64")
+    s.step(int(ref["step"]))
+    m = s.macro()
+    for k in ("rho", "ux", "uy", "T"):
+        assert rel_max(m[k], ref[k]) <= 1e-11, (k, rel_max(m[k], ref[k]))
+    # the same as a solver built from the case itself, bit for bit
+    d = Solver(case, "f64")
+    d.step(int(ref["step"]))
+    assert all(np.array_equal(d.macro()[k], m[k]) for k in m)
+    s.close()
+    d.close()
+
+
+def test_fp32_from_mat_within_tolerance(cuda_device, mat_input):
+    p, _, ref = mat_input
+    s = Solver.from_mat(p, "f32")
+    s.step(int(ref["step"]))
+    m = s.macro()
+    for k in ("rho", "T"):
+        assert rel_l2(m[k], ref[k]) <= 1e-5, (k, rel_l2(m[k], ref[k]))
+    s.close()
+
+
+def test_write_mat_holds_the_state(cuda_device, mat_input, tmp_path):
+    p, _, _ = mat_input
+    s = Solver.from_mat(p, "f64")
+    s.step(3)
+    out = tmp_path / "state.mat"
+    s.write_mat(out, with_dist=True)
+    m = sio.loadmat(str(out))
+    got = s.macro()
+    for k in ("rho", "ux", "uy", "p", "T"):
+        assert np.array_equal(m[k], got[k].T), k
+    f, h = s.dist()
+    assert np.array_equal(m["f"], np.transpose(f.reshape(s.nx, s.ny, 13), (2, 1, 0)))
+    assert np.array_equal(m["h"], np.transpose(h.reshape(s.nx, s.ny, 13), (2, 1, 0)))
+    assert m["t"].item() == pytest.approx(3 * s.dt)
+    s.close()

@@ -11,8 +11,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = [os.path.join(HERE, "csrc", f) for f in ("lbm_kernels.cu", "lbm_engine.cu", "lbm_noalloc.cu", "lbm_server.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("lbm_device.cuh", "lbm_kernels.h", "lbm_host.h", "lbm_common.h", "tma.cuh")] + [
+SRC = [os.path.join(HERE, "csrc", f) for f in ("lbm_kernels.cu", "lbm_engine.cu", "lbm_noalloc.cu", "lbm_server.cu", "lbm_mat.cpp")]
+DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("lbm_device.cuh", "lbm_kernels.h", "lbm_host.h", "lbm_common.h", "lbm_mat.h", "tma.cuh")] + [
     os.path.join(ROOT, "include", "uq_lbm.h")]
 LIB = os.path.join(HERE, "lib", "libuqlbm.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -36,7 +36,7 @@ def build(force=False, verbose=False):
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     cmd = [nvcc(), "-std=c++17", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-shared",
            "-Xcompiler", "-fvisibility=hidden", "-I" + os.path.join(ROOT, "include"),
-           "-o", LIB + ".tmp", *SRC]
+           "-o", LIB + ".tmp", *SRC, "-lz"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

@@ -44,6 +44,7 @@ struct SampleParams {
     // (rho0, 0, 0, T0); rho0 = shref = 0 (full storage) on the FP64 path.
     double rho0, T0n, shref;  // T0n = T0 / Tc
     double inv_mu, two_over_bR;
+    int wide;  // FP32 WENO5 weights in the range-safe form (see weno5)
 };
 
 struct Tile {
@@ -444,8 +445,12 @@ __device__ __forceinline__ float face_div(float n, float d) { return __fdividef(
 // WENO5 (cpuLBM.cpp:1358-1403): Jiang-Shu indicators b_k, linear weights
 // 1/10, 6/10, 3/10, epsilon 1e-6, on |e| times the upwind-ordered values.
 // The nonlinear weights d_k/(eps+b_k)^2 normalised by their sum are formed
-// as d_k prod_{j!=k} (eps+b_j)^2 over the same sum, one division per face.
-template <class C>
+// as d_k prod_{j!=k} (eps+b_j)^2 over the same sum (one division per face).
+// That fourth power (times the candidate values in the numerator) leaves
+// the FP32 range on dimensional data; for samples whose scales allow that
+// (SampleParams::wide, set on the host) the FP32 weights are formed as
+// d_k (m/(eps+b_k))^2 instead, m the smallest eps+b_j, each ratio in (0, 1].
+template <class C, bool WIDE = false>
 __device__ __forceinline__ C weno5(C ae, C s0, C s1, C s2, C s3, C s4)
 {
     const C q0 = xmul(ae, s0), q1 = xmul(ae, s1), q2 = xmul(ae, s2), q3 = xmul(ae, s3), q4 = xmul(ae, s4);
@@ -460,13 +465,40 @@ __device__ __forceinline__ C weno5(C ae, C s0, C s1, C s2, C s3, C s4)
     const C a0 = xfma(xmul(C(13.0 / 12.0), d0), d0, xfma(xmul(C(0.25), l0), l0, C(1e-6)));
     const C a1 = xfma(xmul(C(13.0 / 12.0), d1), d1, xfma(xmul(C(0.25), l1), l1, C(1e-6)));
     const C a2 = xfma(xmul(C(13.0 / 12.0), d2), d2, xfma(xmul(C(0.25), l2), l2, C(1e-6)));
-    const C p0 = xmul(a0, a0), p1 = xmul(a1, a1), p2 = xmul(a2, a2);
-    const C w0 = xmul(C(0.1), xmul(p1, p2)), w1 = xmul(C(0.6), xmul(p0, p2)), w2 = xmul(C(0.3), xmul(p0, p1));
+    C w0, w1, w2;
+    if (sizeof(C) == 4 && WIDE) {
+        const C m = fmin(a0, fmin(a1, a2));
+        const C s0 = __fdividef(m, a0), s1 = __fdividef(m, a1), s2 = __fdividef(m, a2);
+        w0 = xmul(C(0.1), xmul(s0, s0));
+        w1 = xmul(C(0.6), xmul(s1, s1));
+        w2 = xmul(C(0.3), xmul(s2, s2));
+    } else {
+        const C p0 = xmul(a0, a0), p1 = xmul(a1, a1), p2 = xmul(a2, a2);
+        w0 = xmul(C(0.1), xmul(p1, p2));
+        w1 = xmul(C(0.6), xmul(p0, p2));
+        w2 = xmul(C(0.3), xmul(p0, p1));
+    }
     // candidate reconstructions (times 6)
     const C r0 = xfma(C(11), q2, xfma(C(-7), q1, xmul(C(2), q0)));
     const C r1 = xfma(C(2), q3, xfma(C(5), q2, -q1));
     const C r2 = xsub(xfma(C(5), q3, xmul(C(2), q2)), q4);
     return face_div(xfma(w2, r2, xfma(w1, r1, xmul(w0, r0))), xmul(C(6), xadd(xadd(w0, w1), w2)));
+}
+
+// the range-safe form out of line: the general paths that choose the form
+// at run time keep one inlined WENO5 (their code stays compact)
+template <class C>
+__device__ __noinline__ C weno5_wide(C ae, C s0, C s1, C s2, C s3, C s4)
+{
+    return weno5<C, true>(ae, s0, s1, s2, s3, s4);
+}
+
+// WENO5 with the weight form of the sample
+template <class C>
+__device__ __forceinline__ C weno5_sp(const SampleParams &sp, C ae, C s0, C s1, C s2, C s3, C s4)
+{
+    if (sizeof(C) == 4 && sp.wide) return weno5_wide<C>(ae, s0, s1, s2, s3, s4);
+    return weno5<C, false>(ae, s0, s1, s2, s3, s4);
 }
 
 // view of one sample's stage buffer and node flags
@@ -532,7 +564,7 @@ __device__ __noinline__ C flux_exact(const SampleParams &sp, const StageView<S> 
         for (int j = 0; j < 5; ++j)
             if (j < L && (j == jj || (j == jj - diff))) S5[j] = ext;
     }
-    if (sp.fm) return weno5<C>(ae, S5[0], S5[1], S5[2], S5[3], S5[4]);
+    if (sp.fm) return weno5_sp<C>(sp, ae, S5[0], S5[1], S5[2], S5[3], S5[4]);
     return nnd3<C>(ae, S5[0], S5[1], S5[2]);
 }
 
@@ -556,7 +588,7 @@ __device__ __forceinline__ C flux_wrap(const SampleParams &sp, const StageView<S
         r -= r >= N ? N : 0;
         q[j] = axis == 0 ? (C)ldv(v, p, r, y) : (C)ldv(v, p, x, r);
     }
-    if (sp.fm) return weno5<C>(ae, q[0], q[1], q[2], q[3], q[4]);
+    if (sp.fm) return weno5_sp<C>(sp, ae, q[0], q[1], q[2], q[3], q[4]);
     return nnd3<C>(ae, q[1], q[2], q[3]);
 }
 
@@ -578,7 +610,7 @@ __device__ __forceinline__ C flux_axis(const SampleParams &sp, const StageView<S
     const int stride = axis == 0 ? e : e * v.pitch;
     const S *c0 = v.st + (p * v.plane + y * v.pitch + x);
     if (sp.fm) {
-        return weno5<C>(ae, (C)__ldg(c0 - 2 * stride), (C)__ldg(c0 - stride), (C)__ldg(c0), (C)__ldg(c0 + stride),
+        return weno5_sp<C>(sp, ae, (C)__ldg(c0 - 2 * stride), (C)__ldg(c0 - stride), (C)__ldg(c0), (C)__ldg(c0 + stride),
                         (C)__ldg(c0 + 2 * stride));
     }
     return nnd3<C>(ae, (C)__ldg(c0 - stride), (C)__ldg(c0), (C)__ldg(c0 + stride));

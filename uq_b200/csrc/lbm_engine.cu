@@ -8,6 +8,7 @@
 // (CODE/C++/VS2010/simLB/simLB/cpuLBM.cpp:283-450) and the step driver
 // follows runSimStep (main.cpp:32-112).
 #include "lbm_common.h"
+#include "lbm_mat.h"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -226,6 +227,16 @@ void prepare_sample(const HostSample &h, int prec, PreparedSample &out)
     p.c = h.c;
     p.inv_mu = 1.0 / h.mu;
     p.two_over_bR = 2.0 / (h.b * h.R);
+    {
+        // FP32 WENO5 weight form: the division-free form spans (eps + b)^4,
+        // which stays in the float range when |e| c times the stored values
+        // is moderate.  Bound those values by the initial densities and the
+        // energy scale rho R Tc (times generous factors for the polynomials).
+        double rho_max = 0.0;
+        for (double r : h.rho0) rho_max = std::max(rho_max, std::fabs(r));
+        const double scale = 2.0 * h.c * rho_max * std::max(2.0, 10.0 * h.R * h.Tc);
+        p.wide = (prec == LBM_PREC_F32 && !(scale <= 100.0)) ? 1 : 0;
+    }
     // rest state of the stored deviations (FP32 path only)
     if (prec == LBM_PREC_F32) {
         p.rho0 = (h.rho_ref > 0 && std::isfinite(h.rho_ref)) ? h.rho_ref : 1.0;
@@ -814,6 +825,47 @@ lbm_status lbm_create(const lbm_config *cfg, const lbm_init *init, int precision
     lbm_batch_options o{precision, 0, 0, 1};
     h->b.build(1, cfg, init, &o);
     *out = h.release();
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_create_from_mat(const char *path, int precision, lbm_handle **out)
+{
+    API_BEGIN
+    if (!path || !out) throw LbmError(LBM_ERR_INVALID, "null argument");
+    *out = nullptr;
+    MatCase c;
+    mat_read_case(path, c);
+    std::unique_ptr<lbm_handle> h(new lbm_handle);
+    lbm_batch_options o{precision, 0, 0, 1};
+    h->b.build(1, &c.cfg, &c.init, &o);
+    *out = h.release();
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_write_mat(lbm_handle *h, const char *path, int with_dist)
+{
+    API_BEGIN
+    if (!h || !path) throw LbmError(LBM_ERR_INVALID, "null argument");
+    lbm_batch &b = h->b;
+    const HostSample &s = b.hs[0];
+    const size_t n = (size_t)s.nx * s.ny;
+    std::vector<double> rho(n), ux(n), uy(n), T(n), p(n);
+    b.get_macro(0, rho.data(), ux.data(), uy.data(), T.data(), p.data());
+    std::vector<double> f, hh, ex(NQ), ey(NQ);
+    if (with_dist) {
+        f.resize(n * NQ);
+        hh.resize(n * NQ);
+        b.dist_io(0, f.data(), hh.data(), nullptr, nullptr);
+        for (int i = 0; i < NQ; ++i) {
+            ex[i] = s.c * kEX[i];
+            ey[i] = s.c * kEY[i];
+        }
+    }
+    mat_write_fields(path, s.nx, s.ny, rho.data(), ux.data(), uy.data(), p.data(), T.data(), s.step * s.dt, s.dx[0],
+                     s.dy[0], with_dist ? f.data() : nullptr, with_dist ? hh.data() : nullptr,
+                     with_dist ? ex.data() : nullptr, with_dist ? ey.data() : nullptr);
     return LBM_OK;
     API_END
 }

@@ -191,7 +191,7 @@ template <class S, class C>
 __device__ __forceinline__ C line_flux(const SampleParams &sp, const S *__restrict__ c0, int st, C ae)
 {
     if (sp.fm)
-        return weno5<C>(ae, (C)__ldg(c0 - 2 * st), (C)__ldg(c0 - st), (C)__ldg(c0), (C)__ldg(c0 + st),
+        return weno5_sp<C>(sp, ae, (C)__ldg(c0 - 2 * st), (C)__ldg(c0 - st), (C)__ldg(c0), (C)__ldg(c0 + st),
                         (C)__ldg(c0 + 2 * st));
     return nnd3<C>(ae, (C)__ldg(c0 - st), (C)__ldg(c0), (C)__ldg(c0 + st));
 }
@@ -283,11 +283,14 @@ __device__ __forceinline__ void issue_group_load(TileCtx<S, C> &k, int g, int sl
 
 // reconstruction from the staged box (fast path; no solid, no domain edge
 // within the stencil): element step `st` in the box, upwind sign folded in
-// FM: 1 WENO5, 0 NND, -1 the sample's FMETHOD (read at run time)
+// FM: 0 NND, 1 WENO5, 2 WENO5 with the range-safe weights, -1 the
+// sample's FMETHOD and weight form (read at run time)
 template <class S, class C, int FM = -1>
 __device__ __forceinline__ C box_flux(const SampleParams &sp, const S *c0, int st, C ae)
 {
-    if (FM == 1 || (FM < 0 && sp.fm)) return weno5<C>(ae, (C)c0[-2 * st], (C)c0[-st], (C)c0[0], (C)c0[st], (C)c0[2 * st]);
+    if (FM == 1) return weno5<C, false>(ae, (C)c0[-2 * st], (C)c0[-st], (C)c0[0], (C)c0[st], (C)c0[2 * st]);
+    if (FM == 2) return weno5<C, true>(ae, (C)c0[-2 * st], (C)c0[-st], (C)c0[0], (C)c0[st], (C)c0[2 * st]);
+    if (FM < 0 && sp.fm) return weno5_sp<C>(sp, ae, (C)c0[-2 * st], (C)c0[-st], (C)c0[0], (C)c0[st], (C)c0[2 * st]);
     return nnd3<C>(ae, (C)c0[-st], (C)c0[0], (C)c0[st]);
 }
 
@@ -601,7 +604,10 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     sD[NQ * NT + tid] = C(0);
     if (tile_simple(t)) {
         // simple tiles: the flux scheme fixed at compile time (smaller hot code)
-        if (sp.fm) {
+        if (sp.fm && sizeof(S) == 4 && sp.wide) {
+#pragma unroll 1
+            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 2>(k, g);
+        } else if (sp.fm) {
 #pragma unroll 1
             for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 1>(k, g);
         } else {

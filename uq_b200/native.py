@@ -124,6 +124,13 @@ SIGNATURES = {
     "lbm_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(LbmServerStats)]),
     "lbm_server_destroy": (None, [C.c_void_p]),
     "lbm_selftest_bounded_wait": (C.c_int, [C.c_int]),
+    "lbm_mat_read_case": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "lbm_mat_case_get": (C.c_int, [C.c_void_p, C.POINTER(LbmConfig), C.POINTER(LbmInit)]),
+    "lbm_mat_case_free": (None, [C.c_void_p]),
+    "lbm_create_from_mat": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "lbm_mat_write_fields": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double,
+                                       C.c_double, C.c_double, _dp, _dp, _dp, _dp]),
+    "lbm_write_mat": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "lbm_step_noalloc": (C.c_int, [C.POINTER(LbmConfig), C.c_int, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_int,
                                    C.c_void_p]),
 }

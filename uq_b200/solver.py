@@ -52,8 +52,50 @@ class _CaseBuffers:
         self.nx, self.ny = bnd.shape
 
 
+def mat_case(path):
+    """An input MAT file read by the library (loadInput's rules) as a case
+    dict: the lbm_config fields, ``bnd`` [x, y] and the property tables."""
+    L = N.lib()
+    h = C.c_void_p()
+    N.check(L.lbm_mat_read_case(str(path).encode(), C.byref(h)), "lbm_mat_read_case")
+    try:
+        cfg, ini = N.LbmConfig(), N.LbmInit()
+        N.check(L.lbm_mat_case_get(h, C.byref(cfg), C.byref(ini)), "lbm_mat_case_get")
+        case = {name: getattr(cfg, name) for name, _ in N.LbmConfig._fields_ if name not in ("dx_array", "dy_array")}
+        nx, ny, npr = ini.Nx, ini.Ny, ini.numProps
+        case["bnd"] = np.ctypeslib.as_array(ini.bndArray, shape=(nx * ny,)).reshape(nx, ny).copy()
+        case["numProps"] = npr
+        case["cellType"] = np.ctypeslib.as_array(ini.cellType, shape=(npr,)).copy()
+        for k in ("density", "pressure", "temp", "velocityX", "velocityY"):
+            case[k] = np.ctypeslib.as_array(getattr(ini, k), shape=(npr,)).copy()
+        return case
+    finally:
+        L.lbm_mat_case_free(h)
+
+
+def write_mat_fields(path, fields, t=0.0, dx=1.0, dy=1.0, f=None, h=None, ex=None, ey=None):
+    """createMAT's file from host arrays: fields rho, ux, uy, p, T as
+    [x, y] arrays; f, h [x, y, 13] and ex, ey [13] optional."""
+    nx, ny = fields["rho"].shape
+    arrs = [np.ascontiguousarray(fields[k], dtype=np.float64).reshape(-1) for k in ("rho", "ux", "uy", "p", "T")]
+    dist = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (f, h, ex, ey)]
+    ptr = [None if a is None else _d(a) for a in dist]
+    N.check(N.lib().lbm_mat_write_fields(str(path).encode(), nx, ny, *[_d(a) for a in arrs], float(t), float(dx),
+                                         float(dy), *ptr), "lbm_mat_write_fields")
+
+
 class Solver:
     """One solver instance (an ``lbm_handle``): the drop-in for cpuLBM."""
+
+    @classmethod
+    def from_mat(cls, path, precision="f64"):
+        """new cpuLBM(files) on an input MAT file."""
+        return cls(mat_case(path), precision)
+
+    def write_mat(self, path, with_dist=False):
+        """createMAT of the current state (rho, ux, uy, p, T, t, dx, dy; f,
+        h, ex, ey with with_dist)."""
+        N.check(N.lib().lbm_write_mat(self._h, str(path).encode(), 1 if with_dist else 0), "lbm_write_mat")
 
     def __init__(self, case, precision="f64"):
         L = N.lib()
