@@ -70,6 +70,13 @@ typedef struct lbm_config {
     double rho_ref, p_ref, T_ref, Tc_Tref;
     const double *dx_array; /* [Nx] or NULL */
     const double *dy_array; /* [Ny] or NULL */
+    /* Viscosity law of the OpenCL generator (CODE/Python/simLB/codeCL.py:
+     * 986-990; the C++ solver has the constant law only): 0 constant mu
+     * (cpuLBM), 1 VHS mu (T/T_ref)^(0.5 + upsilon), 2 Sutherland
+     * mu (T/T_ref)^(3/2) (T_ref + S_v)/(T + S_v); mu is the viscosity at
+     * T_ref.  A zero-initialised config keeps the constant law. */
+    int mu_model;
+    double upsilon, S_v;
 } lbm_config;
 
 /* Domain: the property-id map and property tables of loadInput

@@ -19,6 +19,8 @@ struct orc {
     int rk, fm;
     int perX, perY, mirN, mirS, mirE, mirW;
     double R, b, K, Tc, mu, Pr, dt, tol;
+    int mu_model;            /* 0 constant, 1 VHS, 2 Sutherland */
+    double visc_exp, S_v, T_ref;
     double ex[NQ], ey[NQ];
     double *dx, *dy;           /* per column / per row cell widths */
     unsigned char *type;       /* [x*Ny+y] cell type */
@@ -163,6 +165,16 @@ static void equilibrium(orc *s, double rho, double ux, double uy, double T, doub
  * tau_h = tau_f/Pr, tau_hf = tau_h tau_f/(tau_f - tau_h). */
 typedef struct macro_s { double rho, ux, uy, T, p, tf, th, thf; } macro_t;
 
+/* dynamic viscosity at temperature T: constant (cpuLBM.cpp:952), VHS or
+ * Sutherland (CODE/Python/simLB/codeCL.py:986-990) */
+static double viscosity(const orc *s, double T)
+{
+    if (s->mu_model == 0) return s->mu;
+    double mu = s->mu * pow(T / s->T_ref, s->visc_exp);
+    if (s->mu_model == 2) mu *= (s->T_ref + s->S_v) / (T + s->S_v);
+    return mu;
+}
+
 static macro_t moments(const orc *s, const double *fv, const double *hv)
 {
     macro_t m;
@@ -180,7 +192,7 @@ static macro_t moments(const orc *s, const double *fv, const double *hv)
     double usq = ax * ax + ay * ay;
     m.T = 2.0 * (sh / r - usq / 2.0) / (s->b * s->R);
     m.p = r * s->R * m.T;
-    m.tf = s->mu / m.p;
+    m.tf = viscosity(s, m.T) / m.p;
     m.th = m.tf / s->Pr;
     m.thf = (m.th * m.tf) / (m.tf - m.th);
     return m;
@@ -541,7 +553,7 @@ static void rk3(orc *s)
             double ax = fabs(m.ux), ay = fabs(m.uy);
             m.T = 2.0 * (sh / r - (ax * ax + ay * ay) / 2.0) / (s->b * s->R);
             m.p = r * s->R * m.T;
-            m.tf = s->mu / m.p;
+            m.tf = viscosity(s, m.T) / m.p;
             m.th = m.tf / s->Pr;
             m.thf = (m.th * m.tf) / (m.tf - m.th);
             Mc[AT(x, y)] = m;
@@ -700,6 +712,9 @@ orc *orc_create(const orc_config *c, const orc_init *in)
     s->mirW = c->mirrorWest;
     s->R = c->R;
     s->mu = c->mu;
+    s->mu_model = c->mu_model;
+    s->visc_exp = c->mu_model == 1 ? 0.5 + c->upsilon : 1.5;
+    s->S_v = c->S_v;
     s->Pr = c->Pr;
     s->tol = c->tol;
 
@@ -712,6 +727,7 @@ orc *orc_create(const orc_config *c, const orc_init *in)
     if (rho_ref == 0) rho_ref = p_ref / (c->R * T_ref);
     else if (p_ref == 0) p_ref = rho_ref * c->R * T_ref;
     else if (T_ref == 0) T_ref = p_ref / (rho_ref * c->R);
+    s->T_ref = T_ref;
 
     s->dx = (double *)malloc(Nx * sizeof(double));
     s->dy = (double *)malloc(Ny * sizeof(double));

@@ -28,6 +28,10 @@ typedef struct orc_config {
     double gamma, R, mu, Pr, dx, dy, Lx, Ly, rho_ref, p_ref, T_ref, Tc_Tref;
     const double *dx_array; /* [Nx] cell widths, or NULL for uniform dx */
     const double *dy_array; /* [Ny] cell heights, or NULL for uniform dy */
+    /* viscosity law of the OpenCL generator (codeCL.py:986-990): 0 constant
+     * mu (the C++ solver), 1 VHS, 2 Sutherland; mu is the value at T_ref */
+    int mu_model;
+    double upsilon, S_v;
 } orc_config;
 
 typedef struct orc_init {

@@ -14,6 +14,8 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 def case_digest(case):
     h = hashlib.sha256()
     for k in sorted(case):
+        if k in ("mu_model", "upsilon", "S_v") and not np.any(np.asarray(case[k])):
+            continue  # the constant viscosity law: as before these keys existed
         h.update(k.encode())
         h.update(np.ascontiguousarray(np.asarray(case[k], dtype=np.float64)).tobytes())
     return h.hexdigest()[:16]

@@ -63,6 +63,8 @@ struct HostSample {
     int flags = 0;
     double R = 1, b = 5, K = 3, Tc = 1, c = 1, mu = 0, Pr = 1, dt = 0, tol = 0;
     double rho_ref = 1, T_ref = 1;  // completed reference state (refineInput)
+    int mu_model = 0;               // viscosity law (lbm_config::mu_model)
+    double upsilon = 0, S_v = 0;
     int nsteps = 0;
     std::vector<double> dx, dy;
     std::vector<uint8_t> type;  // [y*nx + x]

@@ -45,6 +45,10 @@ struct SampleParams {
     double rho0, T0n, shref;  // T0n = T0 / Tc
     double inv_mu, two_over_bR;
     int wide;  // FP32 WENO5 weights in the range-safe form (see weno5)
+    // viscosity law (codeCL.py:986-990): 0 constant mu, 1 VHS, 2 Sutherland;
+    // mu(T) = mu (T/visc_T)^visc_exp [(visc_T + visc_S)/(T + visc_S)]
+    int visc;
+    double visc_exp, visc_S, visc_T;
 };
 
 struct Tile {
@@ -383,7 +387,13 @@ __device__ __forceinline__ Macro macro_from_sums(double r, double rux, double ru
     const double usq = m.ux * m.ux + m.uy * m.uy;
     m.T = (sh * ir - 0.5 * usq) * sp.two_over_bR;
     m.p = r * sp.R * m.T;
-    m.q = m.p * sp.inv_mu;
+    if (sp.visc == 0) {
+        m.q = m.p * sp.inv_mu;  // 1/tau_f = p/mu
+    } else {
+        double mu = sp.mu * pow(m.T / sp.visc_T, sp.visc_exp);
+        if (sp.visc == 2) mu *= (sp.visc_T + sp.visc_S) / (m.T + sp.visc_S);
+        m.q = m.p / mu;
+    }
     return m;
 }
 

@@ -54,6 +54,10 @@ void derive_scalars(const lbm_config &c, int Nx, int Ny, double min_spacing, Sca
     if (c.RKMETHOD < 0 || c.RKMETHOD > 3) throw LbmError(LBM_ERR_INVALID, "RKMETHOD must be 0..3");
     if (c.FMETHOD < 0 || c.FMETHOD > 1) throw LbmError(LBM_ERR_INVALID, "FMETHOD must be 0 (NND) or 1 (WENO5)");
     if (!(c.gamma > 1.0) || !(c.R > 0.0)) throw LbmError(LBM_ERR_INVALID, "gamma must exceed 1 and R be positive");
+    if (c.mu_model < 0 || c.mu_model > 2) throw LbmError(LBM_ERR_INVALID, "mu_model must be 0, 1 or 2");
+    s.mu_model = c.mu_model;
+    s.upsilon = c.upsilon;
+    s.S_v = c.S_v;
     s.rk = c.RKMETHOD;
     s.fm = c.FMETHOD;
     s.flags = (c.periodicX > 0 ? SF_PERX : 0) | (c.periodicY > 0 ? SF_PERY : 0) | (c.mirrorNorth > 0 ? SF_MIRN : 0) |
@@ -144,6 +148,9 @@ HostSample derive(const lbm_config &c, const lbm_init &in)
     s.c = sc.c;
     s.dt = sc.dt;
     s.nsteps = sc.nsteps;
+    s.mu_model = sc.mu_model;
+    s.upsilon = sc.upsilon;
+    s.S_v = sc.S_v;
 
     // property tables completed as refineInput does; per-node initial state
     const int np = in.numProps;
@@ -227,6 +234,10 @@ void prepare_sample(const HostSample &h, int prec, PreparedSample &out)
     p.c = h.c;
     p.inv_mu = 1.0 / h.mu;
     p.two_over_bR = 2.0 / (h.b * h.R);
+    p.visc = h.mu_model;
+    p.visc_exp = h.mu_model == 1 ? 0.5 + h.upsilon : 1.5;
+    p.visc_S = h.S_v;
+    p.visc_T = h.T_ref;
     {
         // FP32 WENO5 weight form: the division-free form spans (eps + b)^4,
         // which stays in the float range when |e| c times the stored values

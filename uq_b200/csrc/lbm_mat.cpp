@@ -285,6 +285,11 @@ void mat_read_case(const char *path, MatCase &c)
     g.p_ref = scalar("p_ref", 0);
     g.T_ref = scalar("T_ref", 0);
     g.Tc_Tref = scalar("Tc_Tref", 0);
+    // optional: the OpenCL generator's viscosity law (absent: constant mu,
+    // as in loadInput)
+    g.mu_model = (int)scalar("mu_model", 0);
+    g.upsilon = scalar("upsilon", 0);
+    g.S_v = scalar("S_v", 0);
     // property tables (cpuLBM.cpp:201-250): max(dims) entries each
     const int np = (int)scalar("numProps", 0);
     auto table = [&](const char *n, std::vector<double> &dst) {

@@ -229,6 +229,10 @@ static lbm_status step_noalloc(const lbm_config *cfg, int Nx, int Ny, const int 
     sp.c = sc.c;
     sp.inv_mu = 1.0 / sc.mu;
     sp.two_over_bR = 2.0 / (sc.b * sc.R);
+    sp.visc = sc.mu_model;
+    sp.visc_exp = sc.mu_model == 1 ? 0.5 + sc.upsilon : 1.5;
+    sp.visc_S = sc.S_v;
+    sp.visc_T = sc.T_ref;
     sp.rho0 = 0.0;
     sp.T0n = 1.0;
     sp.shref = 0.0;

@@ -40,6 +40,7 @@ class LbmConfig(C.Structure):
         ("dx", C.c_double), ("dy", C.c_double), ("Lx", C.c_double), ("Ly", C.c_double),
         ("rho_ref", C.c_double), ("p_ref", C.c_double), ("T_ref", C.c_double), ("Tc_Tref", C.c_double),
         ("dx_array", _dp), ("dy_array", _dp),
+        ("mu_model", C.c_int), ("upsilon", C.c_double), ("S_v", C.c_double),
     ]
 
 

@@ -31,6 +31,7 @@ BASE = dict(
     steps=0, tol=0.0, periodicX=0, periodicY=0, mirrorNorth=0, mirrorSouth=0,
     mirrorEast=0, mirrorWest=0, gamma=1.4, R=1.0, mu=0.05, Pr=0.71, dx=1.0, dy=1.0,
     Lx=0.0, Ly=0.0, rho_ref=1.0, p_ref=1.0, T_ref=1.0, Tc_Tref=1.0, nPrintOut=1 << 30, MAT=0,
+    mu_model=0, upsilon=0.0, S_v=0.0,
 )
 
 
