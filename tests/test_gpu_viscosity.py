@@ -14,7 +14,7 @@ LAWS = [dict(mu_model=1, upsilon=0.25), dict(mu_model=2, S_v=0.4)]
 
 
 def _cases(law):
-    a = W.random_state(24, 20, seed=31, bc="mixed", dT=0.3, solid_frac=0.1, steps=12, du=0.05)
+    a = W.random_state(24, 20, seed=31, bc="mixed", dT=0.1, solid_frac=0.1, steps=12, du=0.02, drho=0.05)
     b = W.couette(nx=24, ny=20, steps=12, seed=9, T_w=1.2)
     for c in (a, b):
         c.update(law)
