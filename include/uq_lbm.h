@@ -168,6 +168,13 @@ LBM_API lbm_status lbm_mat_write_fields(const char *path, int Nx, int Ny, const 
                                         const double *ey);
 /* createMAT(name, DF) of a handle's current state (t = step * dt). */
 LBM_API lbm_status lbm_write_mat(lbm_handle *h, const char *path, int with_dist);
+/* Checkpoint/resume, which the reference cannot do (it only dumps): f, h
+ * and t of a file lbm_write_mat wrote with with_dist = 1 (no GPU needed;
+ * f, h [(x*Ny + y)*13 + i], any pointer may be NULL) ... */
+LBM_API lbm_status lbm_mat_read_dist(const char *path, int Nx, int Ny, double *f, double *h, double *t);
+/* ... and into a handle of the same case: its f, h and step count
+ * (round(t / dt)) become the checkpoint's. */
+LBM_API lbm_status lbm_restore_mat(lbm_handle *h, const char *path);
 
 /* -------------------------------------------------------------- batches
  * Many independent samples (uneven grids, own parameters) advanced

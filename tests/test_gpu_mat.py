@@ -67,3 +67,29 @@ def test_write_mat_holds_the_state(cuda_device, mat_input, tmp_path):
     assert np.array_equal(m["h"], np.transpose(h.reshape(s.nx, s.ny, 13), (2, 1, 0)))
     assert m["t"].item() == pytest.approx(3 * s.dt)
     s.close()
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_resume_from_mat_checkpoint(cuda_device, tmp_path, precision):
+    # run 6 steps, checkpoint, 6 more; a second solver restored from the
+    # checkpoint must continue bit for bit (FP64) or to FP32 storage (f32)
+    from uq_b200 import workloads as W
+
+    case = W.couette(nx=40, ny=24, steps=12, seed=17)
+    a = Solver(case, precision)
+    a.step(6)
+    ck = tmp_path / "ckpt.mat"
+    a.write_mat(ck, with_dist=True)
+    a.step(6)
+    b = Solver(case, precision)
+    b.restore_mat(ck)
+    assert b.step_count == 6
+    b.step(6)
+    fa, ha = a.dist()
+    fb, hb = b.dist()
+    if precision == "f64":
+        assert np.array_equal(fa, fb) and np.array_equal(ha, hb)
+    else:
+        assert rel_l2(fa, fb) <= 1e-6 and rel_l2(ha, hb) <= 1e-6
+    a.close()
+    b.close()

@@ -15,7 +15,7 @@ import pytest
 
 from uq_b200 import native as N
 from uq_b200 import workloads as W
-from uq_b200.solver import mat_case, write_mat_fields
+from uq_b200.solver import mat_case, read_mat_dist, write_mat_fields
 
 from golden_util import GOLDEN, rel_max
 
@@ -130,3 +130,20 @@ def test_oracle_on_the_reference_input():
     m = o.macro()
     for k in ("rho", "ux", "uy", "T"):
         assert rel_max(m[k], ref[k]) <= 1e-11, (k, rel_max(m[k], ref[k]))
+
+
+def test_checkpoint_distributions_round_trip(tmp_path):
+    nx, ny = 11, 6
+    rng = np.random.default_rng(4)
+    fields = {k: rng.standard_normal((nx, ny)) for k in ("rho", "ux", "uy", "p", "T")}
+    f, h = rng.standard_normal((nx, ny, 13)), rng.standard_normal((nx, ny, 13))
+    p = tmp_path / "ckpt.mat"
+    write_mat_fields(p, fields, t=1.75, f=f, h=h, ex=np.zeros(13), ey=np.zeros(13))
+    f2, h2, t = read_mat_dist(p, nx, ny)
+    assert np.array_equal(f2, f) and np.array_equal(h2, h) and t == 1.75
+    with pytest.raises(N.LbmError) as e:  # wrong shape
+        read_mat_dist(p, ny, nx)
+    assert e.value.code == N.LBM_ERR_INVALID
+    write_mat_fields(p, fields)  # no distributions in the file
+    with pytest.raises(N.LbmError):
+        read_mat_dist(p, nx, ny)

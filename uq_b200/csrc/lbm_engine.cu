@@ -881,6 +881,22 @@ lbm_status lbm_write_mat(lbm_handle *h, const char *path, int with_dist)
     API_END
 }
 
+lbm_status lbm_restore_mat(lbm_handle *h, const char *path)
+{
+    API_BEGIN
+    if (!h || !path) throw LbmError(LBM_ERR_INVALID, "null argument");
+    lbm_batch &b = h->b;
+    HostSample &s = b.hs[0];
+    const size_t n = (size_t)s.nx * s.ny * NQ;
+    std::vector<double> f(n), hh(n);
+    double t = 0.0;
+    mat_read_dist(path, s.nx, s.ny, f.data(), hh.data(), &t);
+    b.dist_io(0, nullptr, nullptr, f.data(), hh.data());
+    s.step = (int)std::lround(t / s.dt);
+    return LBM_OK;
+    API_END
+}
+
 void lbm_destroy(lbm_handle *h) { delete h; }
 
 void *lbm_stream(lbm_handle *h) { return h ? (void *)h->b.stream : nullptr; }

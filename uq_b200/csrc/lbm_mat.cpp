@@ -326,6 +326,24 @@ void mat_read_case(const char *path, MatCase &c)
     in.velocityY = c.velocityY.data();
 }
 
+void mat_read_dist(const char *path, int Nx, int Ny, double *f, double *h, double *t)
+{
+    const auto vars = read_mat(path);
+    const size_t n = (size_t)Nx * Ny * 13;
+    const char *names[2] = {"f", "h"};
+    double *dst[2] = {f, h};
+    for (int k = 0; k < 2; ++k) {
+        auto it = vars.find(names[k]);
+        if (it == vars.end()) throw LbmError(LBM_ERR_INVALID, std::string("MAT checkpoint lacks ") + names[k]);
+        const Variable &v = it->second;
+        if (v.dims.size() != 3 || v.dims[0] != 13 || v.dims[1] != (size_t)Ny || v.dims[2] != (size_t)Nx)
+            throw LbmError(LBM_ERR_INVALID, std::string("MAT checkpoint: ") + names[k] + " is not 13 x Ny x Nx");
+        if (dst[k]) std::copy(v.data.begin(), v.data.begin() + n, dst[k]);  // column-major = [(x*Ny + y)*13 + i]
+    }
+    auto it = vars.find("t");
+    if (t) *t = (it == vars.end() || it->second.data.empty()) ? 0.0 : it->second.data[0];
+}
+
 void mat_write_fields(const char *path, int Nx, int Ny, const double *rho, const double *ux, const double *uy,
                       const double *p, const double *T, double t, double dx, double dy, const double *f,
                       const double *h, const double *ex, const double *ey)
@@ -417,6 +435,15 @@ LBM_API lbm_status lbm_mat_case_get(const lbm_mat_case *c, lbm_config *cfg, lbm_
 }
 
 LBM_API void lbm_mat_case_free(lbm_mat_case *c) { delete c; }
+
+LBM_API lbm_status lbm_mat_read_dist(const char *path, int Nx, int Ny, double *f, double *h, double *t)
+{
+    MAT_BEGIN
+    if (!path || Nx < 1 || Ny < 1) throw LbmError(LBM_ERR_INVALID, "bad argument");
+    mat_read_dist(path, Nx, Ny, f, h, t);
+    return LBM_OK;
+    MAT_END
+}
 
 LBM_API lbm_status lbm_mat_write_fields(const char *path, int Nx, int Ny, const double *rho, const double *ux,
                                         const double *uy, const double *p, const double *T, double t, double dx,

@@ -20,6 +20,10 @@ struct MatCase {
 // entries, bndArray with Nx = dims[1], Ny = dims[0] and y flipped.
 void mat_read_case(const char *path, MatCase &c);
 
+// f and h ({13, Ny, Nx}, i.e. [(x*Ny + y)*13 + i]) and t of a file that
+// mat_write_fields wrote with distributions: the checkpoint to resume from.
+void mat_read_dist(const char *path, int Nx, int Ny, double *f, double *h, double *t);
+
 // cpuLBM::createMAT's variables; f, h, ex, ey all non-null adds the
 // distributions.
 void mat_write_fields(const char *path, int Nx, int Ny, const double *rho, const double *ux, const double *uy,

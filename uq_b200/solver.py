@@ -73,6 +73,13 @@ def mat_case(path):
         L.lbm_mat_case_free(h)
 
 
+def read_mat_dist(path, nx, ny):
+    """(f, h, t) of a checkpoint MAT file; f, h as [x, y, 13]."""
+    f, h, t = np.empty(nx * ny * 13), np.empty(nx * ny * 13), C.c_double()
+    N.check(N.lib().lbm_mat_read_dist(str(path).encode(), nx, ny, _d(f), _d(h), C.byref(t)), "lbm_mat_read_dist")
+    return f.reshape(nx, ny, 13), h.reshape(nx, ny, 13), t.value
+
+
 def write_mat_fields(path, fields, t=0.0, dx=1.0, dy=1.0, f=None, h=None, ex=None, ey=None):
     """createMAT's file from host arrays: fields rho, ux, uy, p, T as
     [x, y] arrays; f, h [x, y, 13] and ex, ey [13] optional."""
@@ -96,6 +103,11 @@ class Solver:
         """createMAT of the current state (rho, ux, uy, p, T, t, dx, dy; f,
         h, ex, ey with with_dist)."""
         N.check(N.lib().lbm_write_mat(self._h, str(path).encode(), 1 if with_dist else 0), "lbm_write_mat")
+
+    def restore_mat(self, path):
+        """Resume from a file write_mat(path, with_dist=True) made: f, h and
+        the step count."""
+        N.check(N.lib().lbm_restore_mat(self._h, str(path).encode()), "lbm_restore_mat")
 
     def __init__(self, case, precision="f64"):
         L = N.lib()
