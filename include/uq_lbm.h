@@ -229,7 +229,8 @@ LBM_API void lbm_batch_destroy(lbm_batch *b);
  * No single counterpart in the reference, whose driver runs one solve per
  * process (main.cpp:32-112).  A server owns a device arena carved from the
  * free HBM when it is created and a thread that runs solves submitted at
- * any time, as a continuous batch:
+ * any time, as a continuous batch (the smallest resident solves take
+ * several steps per server step, so that large ones do not pace them):
  *   - a submitted solve waits in a FIFO queue until a region of the arena
  *     large enough for its f, h and stage buffers is free, then joins the
  *     resident set at the next step boundary;
@@ -258,6 +259,9 @@ typedef struct lbm_server_options {
     int max_queued;       /* most solves waiting; 0: no limit */
     int use_graph;        /* replay steps from a CUDA graph while the resident set is unchanged */
     int status_poll_steps;/* steps between reads of the device status words; 0: 32 */
+    int fast_lane_steps;  /* steps per server step of the smallest solves
+                             (each at most 1/16 of the resident nodes, together
+                             at most 1/4); 0: 4; 1: every solve takes one */
 } lbm_server_options;
 
 enum { LBM_REQ_QUEUED = 0, LBM_REQ_RESIDENT = 1, LBM_REQ_DONE = 2 };

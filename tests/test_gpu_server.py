@@ -189,3 +189,30 @@ def test_fragmented_arena_is_compacted(cuda_device):
         for f in FIELDS:
             assert np.array_equal(got[f], ref[f]), (rid, f)
     srv.close()
+
+
+def test_fast_lane_small_solves_take_several_steps(cuda_device):
+    # one large solve paces the batch; the small ones (each < 1/16 of the
+    # resident nodes) take 4 steps per server step and still end exactly
+    # on their step counts with the results they have alone
+    big = W.couette(nx=256, ny=256, steps=600, seed=21)
+    small = [W.couette(nx=32, ny=32, steps=97 + 10 * k, seed=22 + k, fmethod=k % 2, rkmethod=(k // 2) % 2)
+             for k in range(4)]
+    srv = Server(precision="f32", use_graph=True)
+    ids = [srv.submit(big)] + [srv.submit(c) for c in small]
+    for rid in ids:
+        assert srv.wait(rid, timeout=120.0)
+    for rid, case in zip(ids[1:], small):
+        info = srv.info(rid)
+        assert info["steps_done"] == case["steps"]
+        server_steps = info["step_done"] - info["step_admit"]
+        assert server_steps < case["steps"] / 2, (server_steps, case["steps"])
+        code, got = srv.result(rid)
+        st, ref = _alone(case, "f32")
+        assert code == st == N.LBM_OK
+        for f in FIELDS:
+            assert np.array_equal(got[f], ref[f]), f
+    code, got = srv.result(ids[0])
+    st, ref = _alone(big, "f32")
+    assert code == st == N.LBM_OK and np.array_equal(got["rho"], ref["rho"])
+    srv.close()

@@ -133,6 +133,7 @@ struct lbm_server {
     int device = 0;
     bool use_graph = true;
     int max_resident = 1024, max_queued = 0, poll_steps = 32;
+    int fast_k = 4;  // steps per server step of the fast set
     size_t es = 4;
     size_t arena_bytes = 0;
     Clock::time_point t0;
@@ -158,6 +159,11 @@ struct lbm_server {
     DevBuf<int> d_status;
     StepLists lists;
     long long packed_nodes = 0;  // lattice nodes of the resident set
+    // fast set: the first n_fast packed solves, whose tiles and walls are
+    // prefixes of every list; fast_lists holds those prefix lengths
+    int n_fast = 0;
+    StepLists fast_lists;
+    long long fast_nodes = 0;
     cudaGraphExec_t graph = nullptr;
     int stable_steps = 0;
     int *pinned_bits = nullptr;  // kSnapRing x max_resident
@@ -199,6 +205,7 @@ struct lbm_server {
         if (opt && opt->max_resident > 0) max_resident = opt->max_resident;
         if (opt && opt->max_queued > 0) max_queued = opt->max_queued;
         if (opt && opt->status_poll_steps > 0) poll_steps = opt->status_poll_steps;
+        if (opt && opt->fast_lane_steps > 0) fast_k = opt->fast_lane_steps;
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1)
             throw LbmError(LBM_ERR_CUDA, "no CUDA device available (this library has no CPU path)");
@@ -407,6 +414,21 @@ struct lbm_server {
         lists.n_walls_all = (int)walls_all.size();
         lists.walls_rk3 = d_walls_rk3.p;
         lists.n_walls_rk3 = (int)walls_rk3.size();
+        fast_lists = lists;
+        for (int m = 0; m < 4; ++m) fast_lists.n_by_rk[m] = 0;
+        fast_lists.n_rk3 = fast_lists.n_walls_all = fast_lists.n_walls_rk3 = 0;
+        fast_nodes = 0;
+        for (int k = 0; k < n_fast; ++k) {
+            const Request *r = packed[k];
+            const int nt = (int)r->tiles.size(), nw = (int)r->ps.walls.size();
+            fast_lists.n_by_rk[r->ps.p.rk] += nt;
+            fast_lists.n_walls_all += nw;
+            if (r->ps.p.rk == 1) {
+                fast_lists.n_rk3 += nt;
+                fast_lists.n_walls_rk3 += nw;
+            }
+            fast_nodes += (long long)r->nx * r->ny;
+        }
         if (graph) {
             CU(cudaGraphExecDestroy(graph));
             graph = nullptr;
@@ -443,10 +465,19 @@ struct lbm_server {
         return a;
     }
 
+    // one server step: every resident solve one step, then the fast set
+    // fast_k - 1 more (the same launches over the lists' prefixes)
     void enqueue_one_step()
     {
-        if (prec == LBM_PREC_F64) enqueue_step_phases<double, double>(args<double>(), lists, stream);
-        else enqueue_step_phases<float, float>(args<float>(), lists, stream);
+        if (prec == LBM_PREC_F64) {
+            enqueue_step_phases<double, double>(args<double>(), lists, stream);
+            for (int j = 1; n_fast && j < fast_k; ++j)
+                enqueue_step_phases<double, double>(args<double>(), fast_lists, stream);
+        } else {
+            enqueue_step_phases<float, float>(args<float>(), lists, stream);
+            for (int j = 1; n_fast && j < fast_k; ++j)
+                enqueue_step_phases<float, float>(args<float>(), fast_lists, stream);
+        }
     }
 
     void step_once()
@@ -595,6 +626,10 @@ struct lbm_server {
                     if (r->steps_done >= r->steps_total || r->bits != 0 || r->cancel) leaving.push_back(r);
                     else staying.push_back(r);
                 }
+                // a fast solve with fewer than fast_k steps left must leave
+                // the fast set before the next server step
+                for (int k = 0; k < n_fast; ++k)
+                    if (packed[k]->steps_total - packed[k]->steps_done < fast_k) rebuild_needed = true;
                 // FIFO admission into free arena regions
                 bool compacted = false;
                 while (!queue.empty() && (int)(staying.size() + joining.size()) < max_resident) {
@@ -638,9 +673,9 @@ struct lbm_server {
             step_once();
             {
                 std::lock_guard<std::mutex> g(mu);
-                for (Request *r : packed) r->steps_done++;
+                for (size_t k = 0; k < packed.size(); ++k) packed[k]->steps_done += (int)k < n_fast ? fast_k : 1;
                 stats.steps++;
-                stats.lattice_updates += packed_nodes;
+                stats.lattice_updates += packed_nodes + (long long)(fast_k - 1) * fast_nodes;
             }
             if (stats.steps % poll_steps == 0) {
                 auto s = enqueue_snapshot();
@@ -675,6 +710,28 @@ struct lbm_server {
         cv_done.notify_all();
     }
 
+    // Order the packing smallest first and choose the fast set: the leading
+    // solves with at least fast_k steps left, each at most 1/16 of the
+    // resident nodes and together at most 1/4 (mu held).
+    void order_fast_locked()
+    {
+        n_fast = 0;
+        if (fast_k <= 1 || packed.size() < 2) return;
+        long long total = 0;
+        for (const Request *r : packed) total += r->nodes;
+        auto eligible = [&](const Request *r) {
+            return r->steps_total - r->steps_done >= fast_k && r->nodes * 16 <= total;
+        };
+        std::stable_sort(packed.begin(), packed.end(), [&](const Request *a, const Request *b) {
+            const bool ea = eligible(a), eb = eligible(b);
+            if (ea != eb) return ea;
+            return a->nodes < b->nodes;
+        });
+        long long sum = 0;
+        while (n_fast < (int)packed.size() && eligible(packed[n_fast]) && (sum + packed[n_fast]->nodes) * 4 <= total)
+            sum += packed[n_fast++]->nodes;
+    }
+
     // step boundary with a membership change: fields of leaving solves into
     // their stage-2 planes, status words of the old packing, the new
     // packing, then the initial state of joining solves
@@ -705,11 +762,13 @@ struct lbm_server {
             std::lock_guard<std::mutex> g(mu);
             packed = staying;
             packed.insert(packed.end(), joining.begin(), joining.end());
+            order_fast_locked();
         }
         repack();
-        for (size_t k = staying.size(); k < packed.size(); ++k) {
-            Request *r = packed[k];
-            init_solve(r, (int)k);
+        for (Request *r : joining) {
+            int k = 0;
+            while (packed[k] != r) ++k;
+            init_solve(r, k);
             // pageable sources are staged when the copy call returns
             std::lock_guard<std::mutex> g(mu);
             r->fields.clear();

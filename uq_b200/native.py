@@ -68,7 +68,7 @@ class LbmBatchOptions(C.Structure):
 class LbmServerOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("tile_x", C.c_int), ("tile_y", C.c_int), ("arena_bytes", C.c_size_t),
                 ("hbm_fraction", C.c_double), ("max_resident", C.c_int), ("max_queued", C.c_int),
-                ("use_graph", C.c_int), ("status_poll_steps", C.c_int)]
+                ("use_graph", C.c_int), ("status_poll_steps", C.c_int), ("fast_lane_steps", C.c_int)]
 
 
 class LbmRequestInfo(C.Structure):

@@ -334,11 +334,11 @@ class Server:
     as one continuous batch on the GPU; results come back per request."""
 
     def __init__(self, precision="f32", tile=(0, 0), arena_bytes=0, hbm_fraction=0.0, max_resident=0,
-                 max_queued=0, use_graph=True, status_poll_steps=0):
+                 max_queued=0, use_graph=True, status_poll_steps=0, fast_lane_steps=0):
         L = N.lib()
         opt = N.LbmServerOptions(N.PREC[precision], int(tile[0]), int(tile[1]), int(arena_bytes),
                                  float(hbm_fraction), int(max_resident), int(max_queued), 1 if use_graph else 0,
-                                 int(status_poll_steps))
+                                 int(status_poll_steps), int(fast_lane_steps))
         h = C.c_void_p()
         N.check(L.lbm_server_create(C.byref(opt), C.byref(h)), "lbm_server_create")
         self._h = h
