@@ -425,6 +425,12 @@ __device__ __forceinline__ C minmod(C a, C b)
 {
     return a * b > C(0) ? (fabs(a) < fabs(b) ? a : b) : C(0);
 }
+// lane-wise on the packed pair (f, h) of one face
+template <>
+__device__ __forceinline__ float2 minmod<float2>(float2 a, float2 b)
+{
+    return make_float2(minmod<float>(a.x, b.x), minmod<float>(a.y, b.y));
+}
 
 // Round-to-nearest operations the compiler may neither fuse nor split:
 // NND and WENO5 are written with them so that every compiled instance (the
@@ -439,18 +445,50 @@ __device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b)
 __device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float xneg(float a) { return -a; }
+__device__ __forceinline__ double xneg(double a) { return -a; }
+__device__ __forceinline__ float xmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double xmin(double a, double b) { return fmin(a, b); }
+// The same operations on a packed pair of FP32 values (the f and h planes
+// of one face), one sm_100 f32x2 instruction each: every lane is rounded
+// exactly as the scalar operation rounds it, so a face reconstructed in
+// pairs equals the scalar reconstruction bit for bit.  a - b is formed as
+// fma(b, -1, a), which is a - b correctly rounded.
+__device__ __forceinline__ float2 xmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 xadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 xsub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 xfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 xneg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 xmin(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+
+// a constant in the arithmetic type (both lanes of a pair)
+template <class C>
+__device__ __forceinline__ C kc(double v) { return C(v); }
+template <>
+__device__ __forceinline__ float2 kc<float2>(double v) { return make_float2((float)v, (float)v); }
+// FP32 arithmetic, scalar or packed
+template <class C>
+struct IsF32 { static constexpr bool value = false; };
+template <>
+struct IsF32<float> { static constexpr bool value = true; };
+template <>
+struct IsF32<float2> { static constexpr bool value = true; };
 
 // NND (cpuLBM.cpp:1328-1356) on the 3 upwind-ordered values s0, s1, s2
 template <class C>
 __device__ __forceinline__ C nnd3(C ae, C s0, C s1, C s2)
 {
     const C c = xmul(ae, s1);
-    return xfma(C(0.5), minmod<C>(xfma(ae, s2, -c), xfma(-ae, s0, c)), c);
+    return xfma(kc<C>(0.5), minmod<C>(xfma(ae, s2, xneg(c)), xfma(xneg(ae), s0, c)), c);
 }
 
 // one division per face (the FP64 path keeps it correctly rounded)
 __device__ __forceinline__ double face_div(double n, double d) { return n / d; }
 __device__ __forceinline__ float face_div(float n, float d) { return __fdividef(n, d); }
+__device__ __forceinline__ float2 face_div(float2 n, float2 d)
+{
+    return make_float2(__fdividef(n.x, d.x), __fdividef(n.y, d.y));
+}
 
 // WENO5 (cpuLBM.cpp:1358-1403): Jiang-Shu indicators b_k, linear weights
 // 1/10, 6/10, 3/10, epsilon 1e-6, on |e| times the upwind-ordered values.
@@ -465,34 +503,34 @@ __device__ __forceinline__ C weno5(C ae, C s0, C s1, C s2, C s3, C s4)
 {
     const C q0 = xmul(ae, s0), q1 = xmul(ae, s1), q2 = xmul(ae, s2), q3 = xmul(ae, s3), q4 = xmul(ae, s4);
     // second differences d_k and one-sided slopes l_k of the three stencils
-    const C d0 = xfma(C(-2), q1, xadd(q0, q2));
-    const C d1 = xfma(C(-2), q2, xadd(q1, q3));
-    const C d2 = xfma(C(-2), q3, xadd(q2, q4));
-    const C l0 = xfma(C(3), q2, xfma(C(-4), q1, q0));
+    const C d0 = xfma(kc<C>(-2), q1, xadd(q0, q2));
+    const C d1 = xfma(kc<C>(-2), q2, xadd(q1, q3));
+    const C d2 = xfma(kc<C>(-2), q3, xadd(q2, q4));
+    const C l0 = xfma(kc<C>(3), q2, xfma(kc<C>(-4), q1, q0));
     const C l1 = xsub(q1, q3);
-    const C l2 = xfma(C(-4), q3, xfma(C(3), q2, q4));
+    const C l2 = xfma(kc<C>(-4), q3, xfma(kc<C>(3), q2, q4));
     // eps + b_k
-    const C a0 = xfma(xmul(C(13.0 / 12.0), d0), d0, xfma(xmul(C(0.25), l0), l0, C(1e-6)));
-    const C a1 = xfma(xmul(C(13.0 / 12.0), d1), d1, xfma(xmul(C(0.25), l1), l1, C(1e-6)));
-    const C a2 = xfma(xmul(C(13.0 / 12.0), d2), d2, xfma(xmul(C(0.25), l2), l2, C(1e-6)));
+    const C a0 = xfma(xmul(kc<C>(13.0 / 12.0), d0), d0, xfma(xmul(kc<C>(0.25), l0), l0, kc<C>(1e-6)));
+    const C a1 = xfma(xmul(kc<C>(13.0 / 12.0), d1), d1, xfma(xmul(kc<C>(0.25), l1), l1, kc<C>(1e-6)));
+    const C a2 = xfma(xmul(kc<C>(13.0 / 12.0), d2), d2, xfma(xmul(kc<C>(0.25), l2), l2, kc<C>(1e-6)));
     C w0, w1, w2;
-    if (sizeof(C) == 4 && WIDE) {
-        const C m = fmin(a0, fmin(a1, a2));
-        const C s0 = __fdividef(m, a0), s1 = __fdividef(m, a1), s2 = __fdividef(m, a2);
-        w0 = xmul(C(0.1), xmul(s0, s0));
-        w1 = xmul(C(0.6), xmul(s1, s1));
-        w2 = xmul(C(0.3), xmul(s2, s2));
+    if (IsF32<C>::value && WIDE) {
+        const C m = xmin(a0, xmin(a1, a2));
+        const C s0 = face_div(m, a0), s1 = face_div(m, a1), s2 = face_div(m, a2);
+        w0 = xmul(kc<C>(0.1), xmul(s0, s0));
+        w1 = xmul(kc<C>(0.6), xmul(s1, s1));
+        w2 = xmul(kc<C>(0.3), xmul(s2, s2));
     } else {
         const C p0 = xmul(a0, a0), p1 = xmul(a1, a1), p2 = xmul(a2, a2);
-        w0 = xmul(C(0.1), xmul(p1, p2));
-        w1 = xmul(C(0.6), xmul(p0, p2));
-        w2 = xmul(C(0.3), xmul(p0, p1));
+        w0 = xmul(kc<C>(0.1), xmul(p1, p2));
+        w1 = xmul(kc<C>(0.6), xmul(p0, p2));
+        w2 = xmul(kc<C>(0.3), xmul(p0, p1));
     }
     // candidate reconstructions (times 6)
-    const C r0 = xfma(C(11), q2, xfma(C(-7), q1, xmul(C(2), q0)));
-    const C r1 = xfma(C(2), q3, xfma(C(5), q2, -q1));
-    const C r2 = xsub(xfma(C(5), q3, xmul(C(2), q2)), q4);
-    return face_div(xfma(w2, r2, xfma(w1, r1, xmul(w0, r0))), xmul(C(6), xadd(xadd(w0, w1), w2)));
+    const C r0 = xfma(kc<C>(11), q2, xfma(kc<C>(-7), q1, xmul(kc<C>(2), q0)));
+    const C r1 = xfma(kc<C>(2), q3, xfma(kc<C>(5), q2, xneg(q1)));
+    const C r2 = xsub(xfma(kc<C>(5), q3, xmul(kc<C>(2), q2)), q4);
+    return face_div(xfma(w2, r2, xfma(w1, r1, xmul(w0, r0))), xmul(kc<C>(6), xadd(xadd(w0, w1), w2)));
 }
 
 // the range-safe form out of line: the general paths that choose the form

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 namespace uqlbm {
 
@@ -294,6 +295,27 @@ __device__ __forceinline__ C box_flux(const SampleParams &sp, const S *c0, int s
     return nnd3<C>(ae, (C)c0[-st], (C)c0[0], (C)c0[st]);
 }
 
+// Both planes of one face at once (FP32 simple tiles): cf and ch are the
+// f and h values at the face's node, st the upwind element step.  Each lane
+// takes the scalar reconstruction's operations, so the result is the pair
+// box_flux would return for cf and ch.
+template <class S, int FM>
+__device__ __forceinline__ float2 box_flux2(const S *cf, const S *ch, int st, float ae)
+{
+    const float2 a = make_float2(ae, ae);
+#define UQ_PAIR(j) make_float2((float)cf[(j) * st], (float)ch[(j) * st])
+    if (FM == 1) return weno5<float2, false>(a, UQ_PAIR(-2), UQ_PAIR(-1), UQ_PAIR(0), UQ_PAIR(1), UQ_PAIR(2));
+    if (FM == 2) return weno5<float2, true>(a, UQ_PAIR(-2), UQ_PAIR(-1), UQ_PAIR(0), UQ_PAIR(1), UQ_PAIR(2));
+    return nnd3<float2>(a, UQ_PAIR(-1), UQ_PAIR(0), UQ_PAIR(1));
+#undef UQ_PAIR
+}
+
+// simple FP32 tiles reconstruct the f and h planes of a face as one pair
+template <class C, bool SIMPLE, int FM>
+struct PairFaces {
+    static constexpr bool value = SIMPLE && FM >= 0 && std::is_same<C, float>::value;
+};
+
 // Flux of plane slot fh (0 f, 1 h) of direction i at node (xn, yn), along
 // `axis`: solid nodes answer alpha |e| f; nodes whose stencil stays in the
 // staged box and meets no solid/edge read the box; the rest run the wrapped
@@ -338,7 +360,9 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
     const SampleParams &sp = *k.sp;
     const C c = (C)sp.c;
     const C aex = C(abs(EX)) * c, aey = C(abs(EY)) * c;
-    const int nx_items = SX ? 2 * k.TY : 0, ny_items = SY ? 2 * k.TX : 0;
+    constexpr bool PAIR = PairFaces<C, SIMPLE, FM>::value;
+    constexpr int PER = PAIR ? 1 : 2;  // ring items per edge node (f and h)
+    const int nx_items = SX ? PER * k.TY : 0, ny_items = SY ? PER * k.TX : 0;
     // ring items of this direction start at thread ring0 (0 <= ring0 < NT)
     // and cover every item even when a group has more items than threads
     int r0 = k.tid - ring0;
@@ -348,6 +372,36 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
         const int lx = k.tx + HALO_X, ly = k.ty + HALO_Y;
         const S *cf = box + ly * k.BW + lx;
         const S *ch = cf + k.pstride;
+        if constexpr (PAIR) {
+            if (SX) {
+                const float2 v = box_flux2<S, FM>(cf, ch, SX, aex);
+                sf[k.tid] = v.x;
+                sf[NT + k.tid] = v.y;
+            }
+            if (SY) {
+                const float2 v = box_flux2<S, FM>(cf, ch, SY * k.BW, aey);
+                sf[2 * NT + k.tid] = v.x;
+                sf[3 * NT + k.tid] = v.y;
+            }
+            for (int r = r0; r < nx_items + ny_items; r += NT) {
+                if (r < nx_items) {
+                    const int row = r;
+                    const int bx = (SX > 0 ? -1 : k.TX) + HALO_X, by = row + HALO_Y;
+                    const S *e = box + by * k.BW + bx;
+                    const float2 v = box_flux2<S, FM>(e, e + k.pstride, SX, aex);
+                    ringx[row] = v.x;
+                    ringx[k.TY + row] = v.y;
+                } else {
+                    const int col = r - nx_items;
+                    const int bx = col + HALO_X, by = (SY > 0 ? -1 : k.TY) + HALO_Y;
+                    const S *e = box + by * k.BW + bx;
+                    const float2 v = box_flux2<S, FM>(e, e + k.pstride, SY * k.BW, aey);
+                    ringy[col] = v.x;
+                    ringy[k.TX + col] = v.y;
+                }
+            }
+            return;
+        }
         if (SX) {
             sf[k.tid] = box_flux<S, C, FM>(sp, cf, SX, aex);
             sf[NT + k.tid] = box_flux<S, C, FM>(sp, ch, SX, aex);
@@ -505,7 +559,8 @@ __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
         C *rx = k.ringx + (size_t)(buf * G + m) * 2 * k.TY;
         C *ry = k.ringy + (size_t)(buf * G + m) * 2 * k.TX;
         dir_fluxes<S, C, SIMPLE, FM>(k, i, boxes + (size_t)(2 * m) * k.pstride, sf, rx, ry, ring0);
-        ring0 += (c_EX[i] ? 2 * k.TY : 0) + (c_EY[i] ? 2 * k.TX : 0);
+        constexpr int PER = PairFaces<C, SIMPLE, FM>::value ? 1 : 2;
+        ring0 += (c_EX[i] ? PER * k.TY : 0) + (c_EY[i] ? PER * k.TX : 0);
         while (ring0 >= NT) ring0 -= NT;
     }
     __syncthreads();
