@@ -75,3 +75,18 @@ def test_server_and_selftest_without_gpu_fail_loudly():
     else:
         raise AssertionError("lbm_server_create succeeded without a CUDA device")
     assert native.lib().lbm_selftest_bounded_wait(0) == native.LBM_ERR_CUDA
+
+
+def test_oversized_sample_is_rejected_before_reading_arrays():
+    """Ny * roundup(Nx, 32) above 2^26 nodes is refused (32-bit plane
+    offsets in the kernels); the check comes before any per-node array is
+    read, so the small arrays of this case are never indexed."""
+    from uq_b200.solver import _CaseBuffers
+
+    bufs = _CaseBuffers(W.couette(nx=8, ny=8, steps=1))
+    bufs.ini.Nx, bufs.ini.Ny = 1 << 25, 3
+    h = ctypes.c_void_p()
+    L = native.lib()
+    assert L.lbm_create(ctypes.byref(bufs.cfg), ctypes.byref(bufs.ini), 1, ctypes.byref(h)) == native.LBM_ERR_INVALID
+    assert b"too large" in L.lbm_last_error()
+    assert not h.value

@@ -107,6 +107,9 @@ HostSample derive(const lbm_config &c, const lbm_init &in)
         throw LbmError(LBM_ERR_INVALID, "lbm_init tables missing");
     const int Nx = in.Nx, Ny = in.Ny;
     if (Nx < 3 || Ny < 3) throw LbmError(LBM_ERR_INVALID, "Nx and Ny must be at least 3");
+    // the kernels address a sample's 26 planes with 32-bit offsets
+    if ((long long)Ny * (((long long)Nx + 31) / 32 * 32) > (1ll << 26))
+        throw LbmError(LBM_ERR_INVALID, "sample too large: Ny * roundup(Nx, 32) must be at most 2^26 nodes");
     s.nx = Nx;
     s.ny = Ny;
     // cell widths first: the CFL step uses their minimum

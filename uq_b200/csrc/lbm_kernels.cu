@@ -76,17 +76,20 @@ __global__ void k_init(KArgs<S> a, const double *__restrict__ rho, const double 
 }
 
 // ------------------------------------------------------------------ moments
+// macroPropShort of one node: stn is the node's element in plane 0, the
+// planes sp.plane elements apart (offsets in a sample fit in 32 bits).
 template <class S>
-__device__ __forceinline__ Macro node_macro(const S *__restrict__ st, const SampleParams &sp, long long o)
+__device__ __forceinline__ Macro node_macro(const S *__restrict__ stn, const SampleParams &sp)
 {
+    const int PL = (int)sp.plane;
     double r = 0, rux = 0, ruy = 0, sh = 0;
 #pragma unroll
     for (int i = 0; i < NQ; ++i) {
-        const double fv = (double)st[(long long)i * sp.plane + o];
+        const double fv = (double)stn[i * PL];
         r += fv;
         rux += fv * (sp.c * c_EX[i]);
         ruy += fv * (sp.c * c_EY[i]);
-        sh += (double)st[(long long)(NQ + i) * sp.plane + o];
+        sh += (double)stn[(NQ + i) * PL];
     }
     return macro_from_sums(r, rux, ruy, sh, sp);
 }
@@ -114,11 +117,11 @@ __global__ void __launch_bounds__(256, Stage0Blocks<S>::value) k_stage0(KArgs<S>
     if (RK >= 2) {  // EULER, EULER_EQ: fluxes of the state itself
         if (type == 0)
             for (int p = 0; p < NPL; ++p) b2[(long long)p * sp.plane + o] = st[(long long)p * sp.plane + o];
-        if (a.want_residual && type == 0) a.told[node] = node_macro(st, sp, o).T;
+        if (a.want_residual && type == 0) a.told[node] = node_macro(st + o, sp).T;
         return;
     }
     if (type != 0) return;
-    const Macro m = node_macro(st, sp, o);
+    const Macro m = node_macro(st + o, sp);
     if (a.want_residual) a.told[node] = m.T;
     constexpr bool DEV = sizeof(S) == 4;
     const EqArgs<C, DEV> q(m.rho, m.ux, m.uy, m.T, sp);
@@ -676,9 +679,11 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
 
     double res_part = 0;
     if (active && type == 0) {
-        S *__restrict__ st = a.state + sp.state_off;
-        const S *__restrict__ b2 = a.buf2 + sp.state_off;
-        S *__restrict__ b3 = a.buf3 + sp.state_off;
+        // this node in plane 0 of each buffer; planes PL elements apart
+        S *__restrict__ st = a.state + sp.state_off + o;
+        const S *__restrict__ b2 = a.buf2 + sp.state_off + o;
+        S *__restrict__ b3 = a.buf3 + sp.state_off + o;
+        const int PL = (int)sp.plane;
         const C dt = (C)sp.dt;
         bool final_phase = true;
         double fin_r = 0, fin_sh = 0;  // FP64 sums of the new state (MODE 2)
@@ -693,19 +698,19 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             C rq1, rq3, ux1, uy1, ux3, uy3;
             double rho3;
             {
-                m1 = node_macro(st, sp, o);
+                m1 = node_macro(st, sp);
                 rq1 = (C)m1.q; ux1 = (C)m1.ux; uy1 = (C)m1.uy;
             }
             {
                 double r = 0, rux = 0, ruy = 0, sh = 0;
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) {
-                    const double fv = (double)st[(long long)i * sp.plane + o];
+                    const double fv = (double)st[i * PL];
                     const double Df = (double)sD[i * NT + tid];
                     r += fv - Df;
                     rux += fv * (sp.c * c_EX[i]) - Df * (sp.c * c_EX[i]);
                     ruy += fv * (sp.c * c_EY[i]) - Df * (sp.c * c_EY[i]);
-                    sh += (double)st[(long long)(NQ + i) * sp.plane + o] - (double)sD[(NQ + i) * NT + tid];
+                    sh += (double)st[(NQ + i) * PL] - (double)sD[(NQ + i) * NT + tid];
                 }
                 m3 = macro_from_sums(r, rux, ruy, sh, sp);
                 rq3 = (C)m3.q; ux3 = (C)m3.ux; uy3 = (C)m3.uy;
@@ -721,7 +726,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             const C a2 = hdt * itf2, a3 = hdt * itf3, b2c = hdt * ith2, b3c = hdt * ith3;
             const C ia3 = C(1) / (C(1) + a3), ib3 = C(1) / (C(1) + b3c);
             double sf3 = 0;
-#pragma unroll 1
+#pragma unroll
             for (int fam = 0; fam < 4; ++fam) {
                 C e1f[4], e1h[4], e3f[4], e3h[4];
                 q1.fam(fam, e1f, e1h);
@@ -731,7 +736,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if (k >= n) break;
-                    const long long of = (long long)(i0 + k) * sp.plane + o, oh = (long long)(NQ + i0 + k) * sp.plane + o;
+                    const int of = (i0 + k) * PL, oh = (NQ + i0 + k) * PL;
                     vf[k] = (C)st[of]; vh[k] = (C)st[oh]; vf2[k] = (C)b2[of]; vh2[k] = (C)b2[oh];
                 }
 #pragma unroll
@@ -739,7 +744,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     if (k >= n) break;
                     const int i = i0 + k;
                     sf3 += (double)e3f[k];
-                    const long long of = (long long)i * sp.plane + o, oh = (long long)(NQ + i) * sp.plane + o;
+                    const int of = i * PL, oh = (NQ + i) * PL;
                     const C f = vf[k], h = vh[k], f2 = vf2[k], h2 = vh2[k];
                     const C Df = sD[i * NT + tid], Dh = sD[(NQ + i) * NT + tid];
                     const C exi = (C)(sp.c * c_EX[i]), eyi = (C)(sp.c * c_EY[i]);
@@ -767,12 +772,12 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             for (int half = 0; half < 2; ++half) {
                 S acc[NQ];
 #pragma unroll
-                for (int i = 0; i < NQ; ++i) acc[i] = st[(long long)(half * NQ + i) * sp.plane + o];
+                for (int i = 0; i < NQ; ++i) acc[i] = st[(half * NQ + i) * PL];
                 double sum = 0;
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) {
                     const S v = (S)((C)acc[i] - C(0.5) * sD[(half * NQ + i) * NT + tid]);
-                    st[(long long)(half * NQ + i) * sp.plane + o] = v;
+                    st[(half * NQ + i) * PL] = v;
                     sum += (double)v;
                 }
                 if (half == 0) fin_r = sum;
@@ -780,13 +785,13 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             }
         } else {
             // RK1 update (cpuLBM.cpp:1674-1710), EULER (:2130-2168), EULER_EQ (:2220-2258)
-            const Macro m = node_macro(st, sp, o);
+            const Macro m = node_macro(st, sp);
             constexpr bool DEV = sizeof(S) == 4;
             const EqArgs<C, DEV> q(m.rho, m.ux, m.uy, m.T, sp);
             const C ux = (C)m.ux, uy = (C)m.uy, Pr = (C)sp.Pr;
             const C rtf = dt * (C)m.q, rth = dt * Pr * (C)m.q, rg = (Pr - C(1)) * (C)m.q;  // dt/tau_f, dt/tau_h, 1/tau_hf
             double sf = 0;
-#pragma unroll 1
+#pragma unroll
             for (int fam = 0; fam < 4; ++fam) {
                 C fe[4], he[4];
                 q.fam(fam, fe, he);
@@ -795,7 +800,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if (k >= n) break;
-                    const long long of = (long long)(i0 + k) * sp.plane + o, oh = (long long)(NQ + i0 + k) * sp.plane + o;
+                    const int of = (i0 + k) * PL, oh = (NQ + i0 + k) * PL;
                     vf[k] = (C)st[of]; vh[k] = (C)st[oh];
                     if (MODE == 3) { v1f[k] = (C)b2[of]; v1h[k] = (C)b2[oh]; }
                 }
@@ -804,7 +809,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     if (k >= n) break;
                     const int i = i0 + k;
                     sf += (double)fe[k];
-                    const long long of = (long long)i * sp.plane + o, oh = (long long)(NQ + i) * sp.plane + o;
+                    const int of = i * PL, oh = (NQ + i) * PL;
                     const C f = vf[k], h = vh[k];
                     const C Df = sD[i * NT + tid], Dh = sD[(NQ + i) * NT + tid];
                     const C eu = (C)(sp.c * c_EX[i]) * ux + (C)(sp.c * c_EY[i]) * uy;
@@ -831,7 +836,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             if (a.want_residual) {
                 // macroPropShort of the new state: the residual's T, and the
                 // finiteness / positive-density check
-                const Macro mn = node_macro(st, sp, o);
+                const Macro mn = node_macro(st, sp);
                 if (!(mn.rho > 0.0) || !isfinite(mn.rho) || !isfinite(mn.T) || !isfinite(mn.ux) || !isfinite(mn.uy))
                     atomicOr(&a.status[t.sample], STATUS_NONFINITE);
                 const double d = mn.T - a.told[sp.node_off + o];
@@ -842,8 +847,8 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                 if (MODE != 2) {
 #pragma unroll
                     for (int i = 0; i < NQ; ++i) {
-                        r += (double)st[(long long)i * sp.plane + o];
-                        sh += (double)st[(long long)(NQ + i) * sp.plane + o];
+                        r += (double)st[i * PL];
+                        sh += (double)st[(NQ + i) * PL];
                     }
                 }
                 r += sp.rho0;
@@ -885,7 +890,7 @@ __global__ void k_macro_out(const SampleParams *samples, int s, const S *state, 
     const long long n = (long long)sp.nx * sp.ny;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         const int y = (int)(k % sp.ny), x = (int)(k / sp.ny);
-        const Macro m = node_macro(state + sp.state_off, sp, (long long)y * sp.pitch + x);
+        const Macro m = node_macro(state + sp.state_off + (long long)y * sp.pitch + x, sp);
         out[k] = m.rho;
         out[n + k] = m.ux;
         out[2 * n + k] = m.uy;
