@@ -26,8 +26,10 @@ def test_profile_and_launch_count(cuda_device):
     b = Batch([W.couette(nx=64, ny=48, steps=4, seed=1)], "f32")
     ms = b.profile(2)
     assert ms.shape == (6,) and (ms[:5] >= 0).all() and ms[2] > 0
-    assert b.launches_per_step(False) == 5
-    assert b.launches_per_step(True) == 6
+    # 4 x 3 tiles of 16 x 16, two of them simple: pointwise, walls, stencil
+    # 1 (simple and general kernels), walls, stencil 2 (both), + residual
+    assert b.launches_per_step(False) == 7
+    assert b.launches_per_step(True) == 8
 
 
 def test_tile_shape_does_not_change_results(cuda_device):

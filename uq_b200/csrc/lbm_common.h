@@ -94,15 +94,46 @@ void encode_stage_maps(int prec, const SampleParams &p, unsigned char *buf2, uns
 void check_tile_shape(int x, int y);
 int round_up(int v, int m);
 
+// A run of tiles in a device list.
+struct TileRun {
+    const Tile *p = nullptr;
+    int n = 0;
+};
+
 // Device pointers and lengths of the packed lists one step launches over.
+// The pointwise phase runs over the tiles of each RKMETHOD in sample order;
+// the stencil phases over the same tiles as two runs, the simple tiles and
+// the rest, one kernel per run, each compiled for its kind of tile alone.
 struct StepLists {
-    const Tile *by_rk[4] = {nullptr, nullptr, nullptr, nullptr};
-    int n_by_rk[4] = {0, 0, 0, 0};
-    const Tile *rk3 = nullptr;
-    int n_rk3 = 0;
+    TileRun pointwise[4];              // tiles by RKMETHOD, sample order
+    TileRun simple[4], general[4];     // the same tiles by kind
+    TileRun rk3_simple, rk3_general;   // RK3 tiles (final stencil phase)
     const WallNode *walls_all = nullptr, *walls_rk3 = nullptr;
     int n_walls_all = 0, n_walls_rk3 = 0;
 };
+
+// A device list of n tiles whose first ns are simple, as two runs.
+inline void split_runs(const Tile *p, int n, int ns, TileRun &simple, TileRun &general)
+{
+    simple.p = p;
+    simple.n = ns;
+    general.p = p ? p + ns : nullptr;
+    general.n = n - ns;
+}
+
+// Reorder a host tile list so that its simple tiles come first (each kind
+// keeps its order); returns how many are simple.
+inline int simple_first(std::vector<Tile> &v)
+{
+    return (int)(std::stable_partition(v.begin(), v.end(), [](const Tile &t) { return tile_simple(t); }) - v.begin());
+}
+
+template <class S, class C>
+void stencil_runs(const KArgs<S> &a, int phase, int m, const TileRun &s, const TileRun &g, cudaStream_t st)
+{
+    if (s.n) CU((launch_phase<S, C>(a, phase, m, s.p, s.n, nullptr, 0, st, FLUX_SIMPLE)));
+    if (g.n) CU((launch_phase<S, C>(a, phase, m, g.p, g.n, nullptr, 0, st, FLUX_GENERAL)));
+}
 
 // One step: pointwise stages, walls, first stencil phase, and for RK3 the
 // walls of buffer 3 and the final stencil phase.  ev (optional) receives
@@ -112,25 +143,27 @@ void enqueue_step_phases(const KArgs<S> &a, const StepLists &l, cudaStream_t st,
 {
     if (ev) CU(cudaEventRecord(ev[0], st));
     for (int m = 0; m < 4; ++m)
-        if (l.n_by_rk[m]) CU((launch_phase<S, C>(a, 0, m, l.by_rk[m], l.n_by_rk[m], nullptr, 0, st)));
+        if (l.pointwise[m].n) CU((launch_phase<S, C>(a, 0, m, l.pointwise[m].p, l.pointwise[m].n, nullptr, 0, st)));
     if (ev) CU(cudaEventRecord(ev[1], st));
     CU((launch_phase<S, C>(a, 3, 0, nullptr, 0, l.walls_all, l.n_walls_all, st)));
     if (ev) CU(cudaEventRecord(ev[2], st));
-    for (int m = 0; m < 4; ++m)
-        if (l.n_by_rk[m]) CU((launch_phase<S, C>(a, 1, m, l.by_rk[m], l.n_by_rk[m], nullptr, 0, st)));
+    for (int m = 0; m < 4; ++m) stencil_runs<S, C>(a, 1, m, l.simple[m], l.general[m], st);
     if (ev) CU(cudaEventRecord(ev[3], st));
-    if (l.n_rk3) CU((launch_phase<S, C>(a, 4, 1, nullptr, 0, l.walls_rk3, l.n_walls_rk3, st)));
+    const bool rk3 = l.rk3_simple.n || l.rk3_general.n;
+    if (rk3) CU((launch_phase<S, C>(a, 4, 1, nullptr, 0, l.walls_rk3, l.n_walls_rk3, st)));
     if (ev) CU(cudaEventRecord(ev[4], st));
-    if (l.n_rk3) CU((launch_phase<S, C>(a, 2, 1, l.rk3, l.n_rk3, nullptr, 0, st)));
+    if (rk3) stencil_runs<S, C>(a, 2, 1, l.rk3_simple, l.rk3_general, st);
     if (ev) CU(cudaEventRecord(ev[5], st));
 }
 
 inline int step_launches(const StepLists &l)
 {
     int n = 0;
-    for (int m = 0; m < 4; ++m) n += l.n_by_rk[m] ? 2 : 0;  // pointwise + stencil
+    for (int m = 0; m < 4; ++m)
+        n += (l.pointwise[m].n ? 1 : 0) + (l.simple[m].n ? 1 : 0) + (l.general[m].n ? 1 : 0);
     n += l.n_walls_all ? 1 : 0;
-    if (l.n_rk3) n += (l.n_walls_rk3 ? 1 : 0) + 1;
+    if (l.rk3_simple.n || l.rk3_general.n)
+        n += (l.n_walls_rk3 ? 1 : 0) + (l.rk3_simple.n ? 1 : 0) + (l.rk3_general.n ? 1 : 0);
     return n;
 }
 

@@ -373,7 +373,8 @@ struct lbm_batch {
     std::vector<HostSample> hs;
     std::vector<SampleParams> sp;
     std::vector<Tile> tiles_all, tiles_rk3;
-    std::vector<Tile> tiles_by_rk[4];
+    std::vector<Tile> tiles_by_rk[4], tiles_flux[4];  // by RKMETHOD: sample order, simple first
+    int ns_by_rk[4] = {0, 0, 0, 0}, ns_rk3 = 0;      // leading simple tiles of tiles_flux, tiles_rk3
     std::vector<WallNode> walls_all, walls_rk3;
     std::vector<int> tile_first, tile_count;
     long long total_state = 0, total_nodes = 0, lattice_nodes = 0;
@@ -386,7 +387,7 @@ struct lbm_batch {
     DevBuf<int> status, d_tile_first, d_tile_count;
     DevBuf<SampleParams> d_sp;
     DevBuf<Tile> d_tiles_all, d_tiles_rk3;
-    DevBuf<Tile> d_tiles_by_rk[4];
+    DevBuf<Tile> d_tiles_by_rk[4], d_tiles_flux[4];
     DevBuf<WallNode> d_walls_all, d_walls_rk3;
     DevBuf<CUtensorMap> d_maps;
     DevBuf<double> d_fref;
@@ -426,6 +427,13 @@ struct lbm_batch {
             tile_first.push_back(p.first_tile);
             tile_count.push_back(p.ntile);
         }
+        // the stencil phases take the tiles simple ones first (one kernel
+        // per kind); the pointwise phase keeps the sample order
+        for (int m = 0; m < 4; ++m) {
+            tiles_flux[m] = tiles_by_rk[m];
+            ns_by_rk[m] = simple_first(tiles_flux[m]);
+        }
+        ns_rk3 = simple_first(tiles_rk3);
     }
 
     void upload_tiles()
@@ -433,7 +441,10 @@ struct lbm_batch {
         d_sp.upload(sp, stream);
         d_tiles_all.upload(tiles_all, stream);
         d_tiles_rk3.upload(tiles_rk3, stream);
-        for (int m = 0; m < 4; ++m) d_tiles_by_rk[m].upload(tiles_by_rk[m], stream);
+        for (int m = 0; m < 4; ++m) {
+            d_tiles_by_rk[m].upload(tiles_by_rk[m], stream);
+            d_tiles_flux[m].upload(tiles_flux[m], stream);
+        }
         d_tile_first.upload(tile_first, stream);
         d_tile_count.upload(tile_count, stream);
         partial.alloc(tiles_all.size());
@@ -647,11 +658,10 @@ struct lbm_batch {
     {
         StepLists l;
         for (int m = 0; m < 4; ++m) {
-            l.by_rk[m] = d_tiles_by_rk[m].p;
-            l.n_by_rk[m] = (int)tiles_by_rk[m].size();
+            l.pointwise[m] = TileRun{d_tiles_by_rk[m].p, (int)tiles_by_rk[m].size()};
+            split_runs(d_tiles_flux[m].p, (int)tiles_flux[m].size(), ns_by_rk[m], l.simple[m], l.general[m]);
         }
-        l.rk3 = d_tiles_rk3.p;
-        l.n_rk3 = any_rk3 ? (int)tiles_rk3.size() : 0;
+        if (any_rk3) split_runs(d_tiles_rk3.p, (int)tiles_rk3.size(), ns_rk3, l.rk3_simple, l.rk3_general);
         l.walls_all = d_walls_all.p;
         l.n_walls_all = (int)walls_all.size();
         l.walls_rk3 = d_walls_rk3.p;

@@ -94,6 +94,24 @@ __device__ __forceinline__ Macro node_macro(const S *__restrict__ stn, const Sam
     return macro_from_sums(r, rux, ruy, sh, sp);
 }
 
+// The same from the sample's plane 0 and the node's 64-bit offset o (the
+// form the pointwise kernel keeps: it runs at 64 registers, where per-node
+// pointers cost it more than they save).
+template <class S>
+__device__ __forceinline__ Macro node_macro_at(const S *__restrict__ st, const SampleParams &sp, long long o)
+{
+    double r = 0, rux = 0, ruy = 0, sh = 0;
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+        const double fv = (double)st[(long long)i * sp.plane + o];
+        r += fv;
+        rux += fv * (sp.c * c_EX[i]);
+        ruy += fv * (sp.c * c_EY[i]);
+        sh += (double)st[(long long)(NQ + i) * sp.plane + o];
+    }
+    return macro_from_sums(r, rux, ruy, sh, sp);
+}
+
 // ------------------------------------------------------------------- P0
 // RK: 1 (RK3 stages 1+2), 0 (RK1 stage 1), 2 (EULER / EULER_EQ: copy).
 // Pointwise and memory-bound: the FP32 instances keep 64 registers so that
@@ -117,11 +135,11 @@ __global__ void __launch_bounds__(256, Stage0Blocks<S>::value) k_stage0(KArgs<S>
     if (RK >= 2) {  // EULER, EULER_EQ: fluxes of the state itself
         if (type == 0)
             for (int p = 0; p < NPL; ++p) b2[(long long)p * sp.plane + o] = st[(long long)p * sp.plane + o];
-        if (a.want_residual && type == 0) a.told[node] = node_macro(st + o, sp).T;
+        if (a.want_residual && type == 0) a.told[node] = node_macro_at(st, sp, o).T;
         return;
     }
     if (type != 0) return;
-    const Macro m = node_macro(st + o, sp);
+    const Macro m = node_macro_at(st, sp, o);
     if (a.want_residual) a.told[node] = m.T;
     constexpr bool DEV = sizeof(S) == 4;
     const EqArgs<C, DEV> q(m.rho, m.ux, m.uy, m.T, sp);
@@ -595,7 +613,11 @@ size_t flux_smem_bytes_t(size_t es, int tx, int ty)
 
 // MODE: 1 = RK3 stage 3 (fluxes of buffer 2), 2 = RK3 final (buffer 3),
 // 3 = RK1 update, 4 = EULER update, 5 = EULER_EQ update (buffer 2)
-template <class S, class C, int MODE>
+// PATH (FluxPath): FLUX_SIMPLE / FLUX_GENERAL compile only the code of that
+// kind of tile (the two together are far smaller per kernel than one kernel
+// holding both, which the register allocation of the simple path needs); a
+// block given a tile of the other kind returns at once.
+template <class S, class C, int MODE, int PATH>
 __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
 {
     extern __shared__ __align__(128) unsigned char smem_dyn[];
@@ -616,6 +638,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     __shared__ int s_timeout;
 
     const Tile t = a.tiles[blockIdx.x];
+    if (tile_simple(t) != (PATH == FLUX_SIMPLE)) return;
     const int tid = threadIdx.x;
     constexpr int PH = MODE == 2 ? 2 : 1;
     const CUtensorMap *map = a.tmaps + 2 * t.sample + (PH == 1 ? 0 : 1);
@@ -660,7 +683,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     const int type = k.flag & NF_TYPE;
     sD[tid] = C(0);          // direction 0 streams nothing
     sD[NQ * NT + tid] = C(0);
-    if (tile_simple(t)) {
+    if (PATH == FLUX_SIMPLE) {
         // simple tiles: the flux scheme fixed at compile time (smaller hot code)
         if (sp.fm && sizeof(S) == 4 && sp.wide) {
 #pragma unroll 1
@@ -726,8 +749,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             const C a2 = hdt * itf2, a3 = hdt * itf3, b2c = hdt * ith2, b3c = hdt * ith3;
             const C ia3 = C(1) / (C(1) + a3), ib3 = C(1) / (C(1) + b3c);
             double sf3 = 0;
-#pragma unroll
-            for (int fam = 0; fam < 4; ++fam) {
+            auto family = [&](const int fam) {
                 C e1f[4], e1h[4], e3f[4], e3h[4];
                 q1.fam(fam, e1f, e1h);
                 q3.fam(fam, e3f, e3h);
@@ -761,6 +783,13 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     st[of] = (S)accf;
                     st[oh] = (S)acch;
                 }
+            };
+            if constexpr (sizeof(S) == 4) {
+#pragma unroll
+                for (int fam = 0; fam < 4; ++fam) family(fam);
+            } else {
+#pragma unroll 1
+                for (int fam = 0; fam < 4; ++fam) family(fam);
             }
             if (fabs(sf3 - (rho3 - sp.rho0)) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(rho3))))
                 atomicOr(&a.status[t.sample], STATUS_EQ);
@@ -773,12 +802,13 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                 S acc[NQ];
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) acc[i] = st[(half * NQ + i) * PL];
-                double sum = 0;
+                // NaN / Inf propagate through an FP32 sum as through an FP64 one
+                typename std::conditional<sizeof(S) == 4, float, double>::type sum = 0;
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) {
                     const S v = (S)((C)acc[i] - C(0.5) * sD[(half * NQ + i) * NT + tid]);
                     st[(half * NQ + i) * PL] = v;
-                    sum += (double)v;
+                    sum += v;
                 }
                 if (half == 0) fin_r = sum;
                 else fin_sh = sum;
@@ -791,8 +821,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             const C ux = (C)m.ux, uy = (C)m.uy, Pr = (C)sp.Pr;
             const C rtf = dt * (C)m.q, rth = dt * Pr * (C)m.q, rg = (Pr - C(1)) * (C)m.q;  // dt/tau_f, dt/tau_h, 1/tau_hf
             double sf = 0;
-#pragma unroll
-            for (int fam = 0; fam < 4; ++fam) {
+            auto family = [&](const int fam) {
                 C fe[4], he[4];
                 q.fam(fam, fe, he);
                 const int i0 = fam == 0 ? 0 : 4 * fam - 3, n = fam == 0 ? 1 : 4;
@@ -828,6 +857,13 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     st[of] = (S)fn;
                     st[oh] = (S)hn;
                 }
+            };
+            if constexpr (sizeof(S) == 4) {
+#pragma unroll
+                for (int fam = 0; fam < 4; ++fam) family(fam);
+            } else {
+#pragma unroll 1
+                for (int fam = 0; fam < 4; ++fam) family(fam);
             }
             if (MODE >= 4 && fabs(sf - (m.rho - sp.rho0)) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(m.rho))))
                 atomicOr(&a.status[t.sample], STATUS_EQ);
@@ -890,7 +926,7 @@ __global__ void k_macro_out(const SampleParams *samples, int s, const S *state, 
     const long long n = (long long)sp.nx * sp.ny;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         const int y = (int)(k % sp.ny), x = (int)(k / sp.ny);
-        const Macro m = node_macro(state + sp.state_off + (long long)y * sp.pitch + x, sp);
+        const Macro m = node_macro_at(state + sp.state_off, sp, (long long)y * sp.pitch + x);
         out[k] = m.rho;
         out[n + k] = m.ux;
         out[2 * n + k] = m.uy;
@@ -963,9 +999,21 @@ template cudaError_t launch_set_macro<float>(const SampleParams *, int, float *,
 // phase: 0 pointwise stages, 1 stencil phase over buffer 2, 2 RK3 final
 // stencil phase over buffer 3, 3/4 wall fluxes of buffer 2/3.  rk selects
 // the method of the tiles passed (one method per launch).
+template <class S, class C, int PATH>
+void launch_flux(int mode, const KArgs<S> &k, int ntiles, int NT, size_t sm, cudaStream_t st)
+{
+    switch (mode) {
+    case 1: k_flux<S, C, 1, PATH><<<ntiles, NT, sm, st>>>(k); break;
+    case 2: k_flux<S, C, 2, PATH><<<ntiles, NT, sm, st>>>(k); break;
+    case 3: k_flux<S, C, 3, PATH><<<ntiles, NT, sm, st>>>(k); break;
+    case 4: k_flux<S, C, 4, PATH><<<ntiles, NT, sm, st>>>(k); break;
+    default: k_flux<S, C, 5, PATH><<<ntiles, NT, sm, st>>>(k); break;
+    }
+}
+
 template <class S, class C>
 cudaError_t launch_phase(const KArgs<S> &a, int phase, int rk, const Tile *tiles, int ntiles, const WallNode *walls,
-                         int nwalls, cudaStream_t st)
+                         int nwalls, cudaStream_t st, int path)
 {
     KArgs<S> k = a;
     k.tiles = tiles;
@@ -979,11 +1027,9 @@ cudaError_t launch_phase(const KArgs<S> &a, int phase, int rk, const Tile *tiles
     } else if (phase == 1 || phase == 2) {
         if (!ntiles) return cudaSuccess;
         const size_t sm = flux_smem_bytes_t(sizeof(S), a.tx, a.ty);
-        if (phase == 2) k_flux<S, C, 2><<<ntiles, NT, sm, st>>>(k);
-        else if (rk == 1) k_flux<S, C, 1><<<ntiles, NT, sm, st>>>(k);
-        else if (rk == 0) k_flux<S, C, 3><<<ntiles, NT, sm, st>>>(k);
-        else if (rk == 2) k_flux<S, C, 4><<<ntiles, NT, sm, st>>>(k);
-        else k_flux<S, C, 5><<<ntiles, NT, sm, st>>>(k);
+        const int mode = phase == 2 ? 2 : (rk == 1 ? 1 : (rk == 0 ? 3 : (rk == 2 ? 4 : 5)));
+        if (path != FLUX_GENERAL) launch_flux<S, C, FLUX_SIMPLE>(mode, k, ntiles, NT, sm, st);
+        if (path != FLUX_SIMPLE) launch_flux<S, C, FLUX_GENERAL>(mode, k, ntiles, NT, sm, st);
     } else if (phase == 3 || phase == 4) {
         if (nwalls) k_wall<S, C><<<(nwalls + 127) / 128, 128, 0, st>>>(k, phase == 3 ? a.buf2 : a.buf3, walls, nwalls);
     }
@@ -995,11 +1041,13 @@ cudaError_t prepare_kernels()
 {
     const int maxsm = 200 * 1024;
     cudaError_t e = cudaSuccess;
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+#define UQ_FLUX_SMEM(M, P) \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, M, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+    UQ_FLUX_SMEM(1, FLUX_SIMPLE) UQ_FLUX_SMEM(2, FLUX_SIMPLE) UQ_FLUX_SMEM(3, FLUX_SIMPLE)
+    UQ_FLUX_SMEM(4, FLUX_SIMPLE) UQ_FLUX_SMEM(5, FLUX_SIMPLE)
+    UQ_FLUX_SMEM(1, FLUX_GENERAL) UQ_FLUX_SMEM(2, FLUX_GENERAL) UQ_FLUX_SMEM(3, FLUX_GENERAL)
+    UQ_FLUX_SMEM(4, FLUX_GENERAL) UQ_FLUX_SMEM(5, FLUX_GENERAL)
+#undef UQ_FLUX_SMEM
     return e;
 }
 
@@ -1064,9 +1112,9 @@ cudaError_t launch_residual(const SampleParams *samples, int nsamples, const dou
 }
 
 template cudaError_t launch_phase<double, double>(const KArgs<double> &, int, int, const Tile *, int, const WallNode *,
-                                                  int, cudaStream_t);
+                                                  int, cudaStream_t, int);
 template cudaError_t launch_phase<float, float>(const KArgs<float> &, int, int, const Tile *, int, const WallNode *, int,
-                                                cudaStream_t);
+                                                cudaStream_t, int);
 template cudaError_t prepare_kernels<double, double>();
 template cudaError_t prepare_kernels<float, float>();
 template cudaError_t launch_init<double>(const KArgs<double> &, const double *, const double *, const double *,

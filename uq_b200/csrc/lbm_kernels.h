@@ -47,9 +47,15 @@ struct KArgs {
 #endif
 };
 
+// Which tiles a stencil-phase launch covers: FLUX_SIMPLE and FLUX_GENERAL
+// run the kernel compiled for that kind alone over a list holding only that
+// kind; FLUX_BOTH runs both kernels over a mixed list (each skips the
+// other kind's tiles).
+enum FluxPath { FLUX_BOTH = 0, FLUX_SIMPLE = 1, FLUX_GENERAL = 2 };
+
 template <class S, class C>
 cudaError_t launch_phase(const KArgs<S> &a, int phase, int rk, const Tile *tiles, int ntiles, const WallNode *walls,
-                         int nwalls, cudaStream_t st);
+                         int nwalls, cudaStream_t st, int path = FLUX_BOTH);
 template <class S, class C>
 cudaError_t prepare_kernels();
 size_t flux_smem_bytes(int prec, int tx, int ty);

@@ -148,11 +148,13 @@ struct lbm_server {
     std::vector<Request *> packed;
     std::vector<SampleParams> sp;
     std::vector<Tile> tiles_all, tiles_rk3, tiles_by_rk[4];
+    // stencil-phase lists: the simple tiles of every solve, then the others
+    std::vector<Tile> flux_by_rk[4], gen_rk3, gen_by_rk[4];
     std::vector<WallNode> walls_all, walls_rk3;
     std::vector<double> v_tdx, v_tdy, v_dx, v_dy, v_fref;
     std::vector<CUtensorMap> maps;
     DevBuf<SampleParams> d_sp;
-    DevBuf<Tile> d_tiles_rk3, d_tiles_by_rk[4];
+    DevBuf<Tile> d_tiles_rk3, d_tiles_by_rk[4], d_flux_by_rk[4];
     DevBuf<WallNode> d_walls_all, d_walls_rk3;
     DevBuf<double> d_tdx, d_tdy, d_dx, d_dy, d_fref;
     DevBuf<CUtensorMap> d_maps;
@@ -160,7 +162,8 @@ struct lbm_server {
     StepLists lists;
     long long packed_nodes = 0;  // lattice nodes of the resident set
     // fast set: the first n_fast packed solves, whose tiles and walls are
-    // prefixes of every list; fast_lists holds those prefix lengths
+    // prefixes of every list (of both tile runs); fast_lists holds those
+    // prefixes
     int n_fast = 0;
     StepLists fast_lists;
     long long fast_nodes = 0;
@@ -352,6 +355,9 @@ struct lbm_server {
         tiles_all.clear();
         tiles_rk3.clear();
         for (auto &v : tiles_by_rk) v.clear();
+        gen_rk3.clear();
+        for (auto &v : gen_by_rk) v.clear();
+        for (auto &v : flux_by_rk) v.clear();
         walls_all.clear();
         walls_rk3.clear();
         v_tdx.clear();
@@ -376,7 +382,9 @@ struct lbm_server {
                 t.gid = (int)tiles_all.size() | (lt.gid & TILE_SIMPLE);
                 tiles_all.push_back(t);
                 tiles_by_rk[p.rk].push_back(t);
-                if (p.rk == 1) tiles_rk3.push_back(t);
+                const bool simple = tile_simple(t);
+                (simple ? flux_by_rk[p.rk] : gen_by_rk[p.rk]).push_back(t);
+                if (p.rk == 1) (simple ? tiles_rk3 : gen_rk3).push_back(t);
             }
             for (WallNode w : r->ps.walls) {
                 w.sample = (int)k;
@@ -392,8 +400,17 @@ struct lbm_server {
             sp.push_back(p);
             packed_nodes += (long long)r->nx * r->ny;
         }
+        int ns_by_rk[4], ns_rk3 = (int)tiles_rk3.size();
+        for (int m = 0; m < 4; ++m) {
+            ns_by_rk[m] = (int)flux_by_rk[m].size();
+            flux_by_rk[m].insert(flux_by_rk[m].end(), gen_by_rk[m].begin(), gen_by_rk[m].end());
+        }
+        tiles_rk3.insert(tiles_rk3.end(), gen_rk3.begin(), gen_rk3.end());
         d_sp.upload_keep(sp, stream);
-        for (int m = 0; m < 4; ++m) d_tiles_by_rk[m].upload_keep(tiles_by_rk[m], stream);
+        for (int m = 0; m < 4; ++m) {
+            d_tiles_by_rk[m].upload_keep(tiles_by_rk[m], stream);
+            d_flux_by_rk[m].upload_keep(flux_by_rk[m], stream);
+        }
         d_tiles_rk3.upload_keep(tiles_rk3, stream);
         d_walls_all.upload_keep(walls_all, stream);
         d_walls_rk3.upload_keep(walls_rk3, stream);
@@ -405,26 +422,32 @@ struct lbm_server {
         d_maps.upload_keep(maps, stream);
         lists = StepLists{};
         for (int m = 0; m < 4; ++m) {
-            lists.by_rk[m] = d_tiles_by_rk[m].p;
-            lists.n_by_rk[m] = (int)tiles_by_rk[m].size();
+            lists.pointwise[m] = TileRun{d_tiles_by_rk[m].p, (int)tiles_by_rk[m].size()};
+            split_runs(d_flux_by_rk[m].p, (int)flux_by_rk[m].size(), ns_by_rk[m], lists.simple[m], lists.general[m]);
         }
-        lists.rk3 = d_tiles_rk3.p;
-        lists.n_rk3 = (int)tiles_rk3.size();
+        split_runs(d_tiles_rk3.p, (int)tiles_rk3.size(), ns_rk3, lists.rk3_simple, lists.rk3_general);
         lists.walls_all = d_walls_all.p;
         lists.n_walls_all = (int)walls_all.size();
         lists.walls_rk3 = d_walls_rk3.p;
         lists.n_walls_rk3 = (int)walls_rk3.size();
         fast_lists = lists;
-        for (int m = 0; m < 4; ++m) fast_lists.n_by_rk[m] = 0;
-        fast_lists.n_rk3 = fast_lists.n_walls_all = fast_lists.n_walls_rk3 = 0;
+        for (int m = 0; m < 4; ++m) fast_lists.pointwise[m].n = fast_lists.simple[m].n = fast_lists.general[m].n = 0;
+        fast_lists.rk3_simple.n = fast_lists.rk3_general.n = 0;
+        fast_lists.n_walls_all = fast_lists.n_walls_rk3 = 0;
         fast_nodes = 0;
         for (int k = 0; k < n_fast; ++k) {
             const Request *r = packed[k];
-            const int nt = (int)r->tiles.size(), nw = (int)r->ps.walls.size();
-            fast_lists.n_by_rk[r->ps.p.rk] += nt;
+            int ns = 0;
+            for (const Tile &t : r->tiles) ns += tile_simple(t) ? 1 : 0;
+            const int ng = (int)r->tiles.size() - ns, nw = (int)r->ps.walls.size();
+            const int m = r->ps.p.rk;
+            fast_lists.pointwise[m].n += ns + ng;
+            fast_lists.simple[m].n += ns;
+            fast_lists.general[m].n += ng;
             fast_lists.n_walls_all += nw;
-            if (r->ps.p.rk == 1) {
-                fast_lists.n_rk3 += nt;
+            if (m == 1) {
+                fast_lists.rk3_simple.n += ns;
+                fast_lists.rk3_general.n += ng;
                 fast_lists.n_walls_rk3 += nw;
             }
             fast_nodes += (long long)r->nx * r->ny;
