@@ -585,9 +585,9 @@ def run_ours(args, rank, world, local_rank):
             extra["plain_fp64_mlups_32_samples"] = "error: %s" % exc
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.no_probes:
-        v, cores, kind, wall = cpu_reference_arm(os.cpu_count() or 1, 20, samples)
+        v, cores, kind, wall = cpu_reference_arm(os.cpu_count() or 1, 40, samples)
         cpu = {"value": v, "unit": "MLUPS", "cores": cores, "kind": kind,
-               "sample": "%d processes, each one 64x64 ensemble sample x 20 steps (%.1f s wall)" % (cores, wall)}
+               "sample": "%d processes, each one 64x64 ensemble sample x 40 steps (%.1f s wall)" % (cores, wall)}
 
     launches = b.launches_per_step(False) * args.steps
     b.close()
