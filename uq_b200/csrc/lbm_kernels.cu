@@ -281,6 +281,7 @@ struct TileCtx {
     uint64_t *bars;  // [NSTAGE]
     const CUtensorMap *map;
     int *timed_out;  // shared flag
+    bool wrap_fix;   // general tiles: the box crosses a periodic edge
     int *status;     // this sample's status word
     int NT, TX, TY, BW, BH, tid, tx, ty, x, y, x0, y0, x_end, y_end, o;
     uint8_t flag;
@@ -338,13 +339,14 @@ struct PairFaces {
 };
 
 // Flux of plane slot fh (0 f, 1 h) of direction i at node (xn, yn), along
-// `axis`: solid nodes answer alpha |e| f; nodes whose stencil stays in the
-// staged box and meets no solid/edge read the box; the rest run the wrapped
-// or the exact boundary-aware stencil on global memory.  `mirrored`
-// selects the reflected plane (cFLUX at a mirror boundary).
+// `axis`: solid nodes answer alpha |e| f; nodes whose stencil meets no
+// solid or clamped/mirrored edge read the staged box at (ux, uy), the
+// node's place before a periodic wrap (the box holds the periodic images);
+// the rest run the exact boundary-aware stencil on global memory.
+// `mirrored` selects the reflected plane (cFLUX at a mirror boundary).
 template <class S, class C>
-__device__ __forceinline__ C any_node_flux(TileCtx<S, C> &k, const S *box, int i, int xn, int yn, int fh, int axis,
-                                          bool mirrored, bool in_box)
+__device__ __forceinline__ C any_node_flux(TileCtx<S, C> &k, const S *box, int i, int xn, int yn, int ux, int uy,
+                                          int fh, int axis, bool mirrored, bool in_box)
 {
     const SampleParams &sp = *k.sp;
     const int ev = axis == 0 ? c_EX[i] : c_EY[i];
@@ -358,9 +360,9 @@ __device__ __forceinline__ C any_node_flux(TileCtx<S, C> &k, const S *box, int i
         const C fs = (C)__ldg(k.v.st + (pp * k.v.plane + oo));
         return ae * (fs + k.alpha[oo] * (fs + (C)k.fref[pp]));
     }
-    const uint8_t edge = axis == 0 ? (NF_SOLX | NF_EDGX | NF_WRPX) : (NF_SOLY | NF_EDGY | NF_WRPY);
+    const uint8_t edge = axis == 0 ? (NF_SOLX | NF_EDGX) : (NF_SOLY | NF_EDGY);
     if (in_box && !mirrored && !(fl & edge)) {
-        const int lx = xn - (k.x0 - HALO_X), ly = yn - (k.y0 - HALO_Y);
+        const int lx = ux - (k.x0 - HALO_X), ly = uy - (k.y0 - HALO_Y);
         const S *c0 = box + (size_t)fh * k.pstride + ly * k.BW + lx;
         const int e = ev > 0 ? 1 : -1;
         return box_flux<S, C>(sp, c0, axis == 0 ? e : e * k.BW, ae);
@@ -459,7 +461,7 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
         } else {
             if (SX) {
                 C a, b;
-                if (k.flag & (NF_SOLX | NF_EDGX | NF_WRPX)) {
+                if (k.flag & (NF_SOLX | NF_EDGX)) {
                     a = flux_axis<S, C>(sp, k.v, k.x, k.y, i, 0, k.flag);
                     b = flux_axis<S, C>(sp, k.v, k.x, k.y, NQ + i, 0, k.flag);
                 } else {
@@ -471,7 +473,7 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
             }
             if (SY) {
                 C a, b;
-                if (k.flag & (NF_SOLY | NF_EDGY | NF_WRPY)) {
+                if (k.flag & (NF_SOLY | NF_EDGY)) {
                     a = flux_axis<S, C>(sp, k.v, k.x, k.y, i, 1, k.flag);
                     b = flux_axis<S, C>(sp, k.v, k.x, k.y, NQ + i, 1, k.flag);
                 } else {
@@ -492,8 +494,9 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
                 int m;
                 const int xn = SX > 0 ? k.x0 : k.x_end - 1;
                 const int xr = bc_index(sp, xn, -SX, 0, m);
-                const bool in_box = !m && xr == xn - SX;
-                val = any_node_flux<S, C>(k, box, i, xr, yy, fh, 0, m != 0, in_box);
+                // in the box: the neighbour itself, or its periodic image
+                const bool in_box = !m && (xr == xn - SX || (sp.flags & SF_PERX));
+                val = any_node_flux<S, C>(k, box, i, xr, yy, xn - SX, yy, fh, 0, m != 0, in_box);
             }
             ringx[fh * k.TY + row] = val;
         } else {
@@ -503,8 +506,8 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
                 int m;
                 const int yn = SY > 0 ? k.y0 : k.y_end - 1;
                 const int yr = bc_index(sp, yn, -SY, 1, m);
-                const bool in_box = !m && yr == yn - SY;
-                val = any_node_flux<S, C>(k, box, i, xx, yr, fh, 1, m != 0, in_box);
+                const bool in_box = !m && (yr == yn - SY || (sp.flags & SF_PERY));
+                val = any_node_flux<S, C>(k, box, i, xx, yr, xx, yn - SY, fh, 1, m != 0, in_box);
             }
             ringy[fh * k.TX + col] = val;
         }
@@ -553,6 +556,50 @@ __device__ __forceinline__ void dir_divergence(TileCtx<S, C> &k, const int i, co
     k.sD[(NQ + i) * NT + k.tid] = oh - inh;
 }
 
+// General tiles whose box crosses a periodic edge: the box cells outside
+// the domain along a periodic axis get the periodic images of the staged
+// planes (TMA does not wrap), so wrapped stencils read the box like any
+// other.  Along a non-periodic axis the cells outside stay as loaded; no box
+// path reads them (nodes near such edges take the exact stencil).
+template <int G, class S, class C>
+__device__ void wrap_fixup(TileCtx<S, C> &k, int g, S *boxes)
+{
+    const SampleParams &sp = *k.sp;
+    const bool px = (sp.flags & SF_PERX) != 0, py = (sp.flags & SF_PERY) != 0;
+    const int nx = sp.nx, ny = sp.ny, BW = k.BW, BH = k.BH;
+    const int gx0 = k.x0 - HALO_X, gy0 = k.y0 - HALO_Y;
+    // box columns [0, cl) and [cr, BW) lie outside [0, nx); rows [0, rl), [rr, BH) outside [0, ny)
+    const int cl = px ? max(0, min(BW, -gx0)) : 0, cr = px ? max(cl, min(BW, nx - gx0)) : BW;
+    const int rl = py ? max(0, min(BH, -gy0)) : 0, rr = py ? max(rl, min(BH, ny - gy0)) : BH;
+    const int ncol = cl + (BW - cr), nrow = rl + (BH - rr), inner = cr - cl;
+    // the wrapped columns in every row, then the wrapped rows of the other columns
+    const int n1 = ncol * BH, per = n1 + nrow * inner;
+    for (int e = k.tid; e < 2 * G * per; e += k.NT) {
+        const int pl = e / per, q = e - pl * per;
+        int bx, by;
+        if (q < n1) {
+            const int c = q / BH;
+            by = q - c * BH;
+            bx = c < cl ? c : cr + (c - cl);
+        } else {
+            const int q2 = q - n1, r = q2 / inner;
+            bx = cl + (q2 - r * inner);
+            by = r < rl ? r : rr + (r - rl);
+        }
+        int gx = gx0 + bx, gy = gy0 + by;
+        if (gx < 0 || gx >= nx) {
+            if (!px) continue;
+            gx = ((gx % nx) + nx) % nx;
+        }
+        if (gy < 0 || gy >= ny) {
+            if (!py) continue;
+            gy = ((gy % ny) + ny) % ny;
+        }
+        const int plane = (pl & 1) * NQ + group_dir<G>(g, pl >> 1);
+        boxes[(size_t)pl * k.pstride + by * BW + bx] = ldv(k.v, plane, gx, gy);
+    }
+}
+
 // Group g of G directions: wait for its staged boxes, the face fluxes
 // (posFluxes/computeFlux, cpuLBM.cpp:1405-1500; solid nodes answer
 // wallFluxes' alpha |e| f, cpuLBM.cpp:1576-1586) and edge fluxes of each,
@@ -572,6 +619,11 @@ __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
         atomicOr(k.status, STATUS_TIMEOUT);
     }
     const S *boxes = k.stg + (size_t)slot * 2 * G * k.pstride;
+    if (!SIMPLE && k.wrap_fix) {
+        // k.wrap_fix is the same for the whole block
+        wrap_fixup<G>(k, g, const_cast<S *>(boxes));
+        __syncthreads();
+    }
     int ring0 = 0;
 #pragma unroll 1
     for (int m = 0; m < G; ++m) {
@@ -677,6 +729,9 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     k.tx = tx; k.ty = ty; k.x = x; k.y = y;
     k.x_end = x_end; k.y_end = y_end; k.o = o;
     k.active = active;
+    k.wrap_fix = PATH != FLUX_SIMPLE &&
+                 (((sp.flags & SF_PERX) && (t.x0 < HALO_X || t.x0 + TX + HALO_X > sp.nx)) ||
+                  ((sp.flags & SF_PERY) && (t.y0 < HALO_Y || t.y0 + TY + HALO_Y > sp.ny)));
     k.flag = active ? v.nf[o] : 0;
     k.tdx = active ? (C)a.tdx[sp.xoff + x] : C(0);
     k.tdy = active ? (C)a.tdy[sp.yoff + y] : C(0);
