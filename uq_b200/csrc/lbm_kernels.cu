@@ -338,6 +338,81 @@ struct PairFaces {
     static constexpr bool value = SIMPLE && FM >= 0 && std::is_same<C, float>::value;
 };
 
+// flux_exact (the boundary-aware stencil with the linear extrapolation over
+// a solid edge) for both planes of direction i at node (xn, yn), reading
+// the values from the staged box (fb: the f plane; the h plane pstride
+// further) instead of global memory.  (ux, uy) is the node's place in box
+// coordinates before a periodic wrap.  Every point the stencil and the
+// extrapolation touch lies within 3 nodes of the node along the axis,
+// inside the box; positions come from bc_index as in flux_exact (clamped at
+// a closed edge; along a periodic axis the box holds the images at the
+// unwrapped places).  Not for an axis with a mirror edge (that reads the
+// reflected direction's planes).
+template <class S, class C>
+__device__ __noinline__ void flux_exact_box(const SampleParams &sp, const StageView<S> &v, const S *fb, int pstride,
+                                            int BW, int bx0, int by0, int xn, int yn, int ux, int uy, int i, int axis,
+                                            C &outf, C &outh)
+{
+    const int ev = axis == 0 ? c_EX[i] : c_EY[i];
+    const int e = isgn(ev);
+    const C ae = (C)(sp.c * (double)abs(ev));
+    const bool per = (sp.flags & (axis == 0 ? SF_PERX : SF_PERY)) != 0;
+    const int L = sp.fm ? 5 : 3, low = (L - 1) / 2;
+    const int pos = axis == 0 ? xn : yn, upos = axis == 0 ? ux : uy;
+    const int j1 = pos - e * low, uj1 = upos - e * low;
+    // box element of axis coordinate b (the other coordinate fixed)
+    auto at = [&](int b) { return axis == 0 ? (uy - by0) * BW + (b - bx0) : (b - by0) * BW + (ux - bx0); };
+    C Sf[5], Sh[5];
+    int sld[5];
+    int any = 0;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        if (j < L) {
+            int m;
+            const int r = bc_index(sp, j1, e * j, axis, m);
+            const int o = at(per ? uj1 + e * j : r);
+            Sf[j] = (C)fb[o];
+            Sh[j] = (C)fb[pstride + o];
+            const int xr = axis == 0 ? r : xn, yr = axis == 0 ? yn : r;
+            sld[j] = (v.nf[yr * v.pitch + xr] & NF_TYPE) == 2;
+            any |= sld[j];
+        }
+    }
+    if (any) {
+        int diff = 0, jj = 0, pe = 0, m;
+        for (int j = 0; j < L - 1; ++j) {
+            diff = sld[j] - sld[j + 1];
+            if (diff > 0) { jj = j; pe = bc_index(sp, j1, e * j, axis, m); break; }
+            if (diff < 0) { jj = j + 1; pe = bc_index(sp, j1, e * (j + 1), axis, m); break; }
+        }
+        const int upe = uj1 + e * jj;
+        const int o1 = at(per ? upe + e * diff : bc_index(sp, pe, e * diff, axis, m));
+        const int o2 = at(per ? upe + 2 * e * diff : bc_index(sp, pe, e * 2 * diff, axis, m));
+        const C extf = C(2) * (C)fb[o1] - (C)fb[o2];
+        const C exth = C(2) * (C)fb[pstride + o1] - (C)fb[pstride + o2];
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+            if (j < L && (j == jj || (j == jj - diff))) {
+                Sf[j] = extf;
+                Sh[j] = exth;
+            }
+    }
+    if (sp.fm) {
+        outf = weno5_sp<C>(sp, ae, Sf[0], Sf[1], Sf[2], Sf[3], Sf[4]);
+        outh = weno5_sp<C>(sp, ae, Sh[0], Sh[1], Sh[2], Sh[3], Sh[4]);
+    } else {
+        outf = nnd3<C>(ae, Sf[0], Sf[1], Sf[2]);
+        outh = nnd3<C>(ae, Sh[0], Sh[1], Sh[2]);
+    }
+}
+
+// The axis has a mirror edge (its boundary-aware stencils read reflected
+// planes from global memory).
+__device__ __forceinline__ bool mirror_axis(const SampleParams &sp, int axis)
+{
+    return (sp.flags & (axis == 0 ? (SF_MIRW | SF_MIRE) : (SF_MIRN | SF_MIRS))) != 0;
+}
+
 // Flux of plane slot fh (0 f, 1 h) of direction i at node (xn, yn), along
 // `axis`: solid nodes answer alpha |e| f; nodes whose stencil meets no
 // solid or clamped/mirrored edge read the staged box at (ux, uy), the
@@ -461,7 +536,10 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
         } else {
             if (SX) {
                 C a, b;
-                if (k.flag & (NF_SOLX | NF_EDGX)) {
+                if ((k.flag & (NF_SOLX | NF_EDGX)) && !mirror_axis(sp, 0)) {
+                    flux_exact_box<S, C>(sp, k.v, box, k.pstride, k.BW, k.x0 - HALO_X, k.y0 - HALO_Y, k.x, k.y, k.x,
+                                         k.y, i, 0, a, b);
+                } else if (k.flag & (NF_SOLX | NF_EDGX)) {
                     a = flux_axis<S, C>(sp, k.v, k.x, k.y, i, 0, k.flag);
                     b = flux_axis<S, C>(sp, k.v, k.x, k.y, NQ + i, 0, k.flag);
                 } else {
@@ -473,7 +551,10 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
             }
             if (SY) {
                 C a, b;
-                if (k.flag & (NF_SOLY | NF_EDGY)) {
+                if ((k.flag & (NF_SOLY | NF_EDGY)) && !mirror_axis(sp, 1)) {
+                    flux_exact_box<S, C>(sp, k.v, box, k.pstride, k.BW, k.x0 - HALO_X, k.y0 - HALO_Y, k.x, k.y, k.x,
+                                         k.y, i, 1, a, b);
+                } else if (k.flag & (NF_SOLY | NF_EDGY)) {
                     a = flux_axis<S, C>(sp, k.v, k.x, k.y, i, 1, k.flag);
                     b = flux_axis<S, C>(sp, k.v, k.x, k.y, NQ + i, 1, k.flag);
                 } else {
