@@ -750,11 +750,14 @@ size_t flux_smem_bytes_t(size_t es, int tx, int ty)
 // kind of tile (the two together are far smaller per kernel than one kernel
 // holding both, which the register allocation of the simple path needs); a
 // block given a tile of the other kind returns at once.
-template <class S, class C, int MODE, int PATH>
+// T16: the tile shape is the default 16 x 16, compiled in (box widths,
+// strides and the thread-to-node map become constants); otherwise read from
+// the arguments.
+template <class S, class C, int MODE, int PATH, bool T16>
 __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
 {
     extern __shared__ __align__(128) unsigned char smem_dyn[];
-    const int TX = a.tx, TY = a.ty, NT = TX * TY;
+    const int TX = T16 ? 16 : a.tx, TY = T16 ? 16 : a.ty, NT = TX * TY;
     const int BW = TX + 2 * HALO_X, BH = TY + 2 * HALO_Y;
     constexpr int G = FluxGroup<S>::value;
     constexpr int NST = GroupCfg<G>::NSTAGE;
@@ -1135,16 +1138,23 @@ template cudaError_t launch_set_macro<float>(const SampleParams *, int, float *,
 // phase: 0 pointwise stages, 1 stencil phase over buffer 2, 2 RK3 final
 // stencil phase over buffer 3, 3/4 wall fluxes of buffer 2/3.  rk selects
 // the method of the tiles passed (one method per launch).
+template <class S, class C, int PATH, bool T16>
+void launch_flux_t(int mode, const KArgs<S> &k, int ntiles, int NT, size_t sm, cudaStream_t st)
+{
+    switch (mode) {
+    case 1: k_flux<S, C, 1, PATH, T16><<<ntiles, NT, sm, st>>>(k); break;
+    case 2: k_flux<S, C, 2, PATH, T16><<<ntiles, NT, sm, st>>>(k); break;
+    case 3: k_flux<S, C, 3, PATH, T16><<<ntiles, NT, sm, st>>>(k); break;
+    case 4: k_flux<S, C, 4, PATH, T16><<<ntiles, NT, sm, st>>>(k); break;
+    default: k_flux<S, C, 5, PATH, T16><<<ntiles, NT, sm, st>>>(k); break;
+    }
+}
+
 template <class S, class C, int PATH>
 void launch_flux(int mode, const KArgs<S> &k, int ntiles, int NT, size_t sm, cudaStream_t st)
 {
-    switch (mode) {
-    case 1: k_flux<S, C, 1, PATH><<<ntiles, NT, sm, st>>>(k); break;
-    case 2: k_flux<S, C, 2, PATH><<<ntiles, NT, sm, st>>>(k); break;
-    case 3: k_flux<S, C, 3, PATH><<<ntiles, NT, sm, st>>>(k); break;
-    case 4: k_flux<S, C, 4, PATH><<<ntiles, NT, sm, st>>>(k); break;
-    default: k_flux<S, C, 5, PATH><<<ntiles, NT, sm, st>>>(k); break;
-    }
+    if (k.tx == 16 && k.ty == 16) launch_flux_t<S, C, PATH, true>(mode, k, ntiles, NT, sm, st);
+    else launch_flux_t<S, C, PATH, false>(mode, k, ntiles, NT, sm, st);
 }
 
 template <class S, class C>
@@ -1177,13 +1187,16 @@ cudaError_t prepare_kernels()
 {
     const int maxsm = 200 * 1024;
     cudaError_t e = cudaSuccess;
-#define UQ_FLUX_SMEM(M, P) \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_flux<S, C, M, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+#define UQ_FLUX_SMEM1(M, P, T)                                                                              \
+    if (e == cudaSuccess)                                                                                   \
+        e = cudaFuncSetAttribute(k_flux<S, C, M, P, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+#define UQ_FLUX_SMEM(M, P) UQ_FLUX_SMEM1(M, P, true) UQ_FLUX_SMEM1(M, P, false)
     UQ_FLUX_SMEM(1, FLUX_SIMPLE) UQ_FLUX_SMEM(2, FLUX_SIMPLE) UQ_FLUX_SMEM(3, FLUX_SIMPLE)
     UQ_FLUX_SMEM(4, FLUX_SIMPLE) UQ_FLUX_SMEM(5, FLUX_SIMPLE)
     UQ_FLUX_SMEM(1, FLUX_GENERAL) UQ_FLUX_SMEM(2, FLUX_GENERAL) UQ_FLUX_SMEM(3, FLUX_GENERAL)
     UQ_FLUX_SMEM(4, FLUX_GENERAL) UQ_FLUX_SMEM(5, FLUX_GENERAL)
 #undef UQ_FLUX_SMEM
+#undef UQ_FLUX_SMEM1
     return e;
 }
 
