@@ -448,11 +448,15 @@ __device__ __forceinline__ C any_node_flux(TileCtx<S, C> &k, const S *box, int i
 // Own-node face fluxes of direction i into sf_m (fx_f, fx_h, fy_f, fy_h)
 // and the upwind fluxes across the tile edges into ringx_m / ringy_m
 // (items numbered from ring0 over the block's threads).
-template <class S, class C, bool SIMPLE, int FM>
+// CEX, CEY: the direction's components when fixed at compile time (else
+// DIR_RT and read from the table).
+constexpr int DIR_RT = 99;
+
+template <class S, class C, bool SIMPLE, int FM, int CEX = DIR_RT, int CEY = DIR_RT>
 __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const S *box, C *sf, C *ringx, C *ringy,
                                            int ring0)
 {
-    const int EX = c_EX[i], EY = c_EY[i];
+    const int EX = CEX != DIR_RT ? CEX : c_EX[i], EY = CEY != DIR_RT ? CEY : c_EY[i];
     const int SX = isgn(EX), SY = isgn(EY);
     const int NT = k.NT;
     const SampleParams &sp = *k.sp;
@@ -597,11 +601,11 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
 
 // divergence D = (dt/dx, dt/dy).(F_out - F_in) of cFLUX
 // (cpuLBM.cpp:1436-1470) for direction i at this node
-template <class S, class C>
+template <class S, class C, int CEX = DIR_RT, int CEY = DIR_RT>
 __device__ __forceinline__ void dir_divergence(TileCtx<S, C> &k, const int i, const C *sf, const C *ringx,
                                                const C *ringy)
 {
-    const int SX = isgn(c_EX[i]), SY = isgn(c_EY[i]);
+    const int SX = isgn(CEX != DIR_RT ? CEX : c_EX[i]), SY = isgn(CEY != DIR_RT ? CEY : c_EY[i]);
     const int NT = k.NT;
     C of = C(0), oh = C(0), inf_ = C(0), inh = C(0);
     bool have = false;
@@ -733,6 +737,69 @@ __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
     // every reader of this group has passed.
 }
 
+// Direction m of group g for four directions per group (group_dir<4>), its
+// components as constants (the D2Q13 table: e1..e4 = (1,0) (0,1) (-1,0)
+// (0,-1), e5..e8 = (1,1) (-1,1) (-1,-1) (1,-1), e9..e12 = 2 e1..2 e4).
+template <int g, int m>
+struct Dir4 {
+    static constexpr int i = 4 * g + 1 + (m >> 1) + 2 * (m & 1);
+    static constexpr int EX = m == 0 ? (g == 2 ? 2 : 1)
+                            : m == 1 ? (g == 2 ? -2 : -1)
+                            : m == 2 ? (g == 1 ? -1 : 0)
+                                     : (g == 1 ? 1 : 0);
+    static constexpr int EY = m == 0 ? (g == 1 ? 1 : 0)
+                            : m == 1 ? (g == 1 ? -1 : 0)
+                            : m == 2 ? (g == 2 ? 2 : 1)
+                                     : (g == 2 ? -2 : -1);
+};
+
+template <class S, class C, int FM, int g, int m>
+__device__ __forceinline__ void dir_fluxes_c(TileCtx<S, C> &k, const S *boxes, int &ring0)
+{
+    using D = Dir4<g, m>;
+    const int NT = k.NT;
+    constexpr int b = (g & 1) * 4 + m;
+    dir_fluxes<S, C, true, FM, D::EX, D::EY>(k, D::i, boxes + (size_t)(2 * m) * k.pstride, k.sf + (size_t)b * 4 * NT,
+                                             k.ringx + (size_t)b * 2 * k.TY, k.ringy + (size_t)b * 2 * k.TX, ring0);
+    ring0 += (D::EX ? k.TY : 0) + (D::EY ? k.TX : 0);
+    while (ring0 >= NT) ring0 -= NT;
+}
+
+template <class S, class C, int g, int m>
+__device__ __forceinline__ void dir_divergence_c(TileCtx<S, C> &k)
+{
+    using D = Dir4<g, m>;
+    constexpr int b = (g & 1) * 4 + m;
+    dir_divergence<S, C, D::EX, D::EY>(k, D::i, k.sf + (size_t)b * 4 * k.NT, k.ringx + (size_t)b * 2 * k.TY,
+                                       k.ringy + (size_t)b * 2 * k.TX);
+}
+
+// dir_group for simple tiles with the group fixed at compile time (four
+// directions per group): every direction's components are constants.
+template <class S, class C, int FM, int g>
+__device__ __forceinline__ void dir_group_c(TileCtx<S, C> &k)
+{
+    constexpr int G = 4, NST = GroupCfg<G>::NSTAGE;
+    constexpr int slot = g % NST;
+    constexpr uint32_t parity = (g / NST) & 1;
+    if (!mbar_wait_bounded(&k.bars[slot], parity, TMA_WAIT_POLLS)) {
+        *k.timed_out = 1;
+        atomicOr(k.status, STATUS_TIMEOUT);
+    }
+    const S *boxes = k.stg + (size_t)slot * 2 * G * k.pstride;
+    int ring0 = 0;
+    dir_fluxes_c<S, C, FM, g, 0>(k, boxes, ring0);
+    dir_fluxes_c<S, C, FM, g, 1>(k, boxes, ring0);
+    dir_fluxes_c<S, C, FM, g, 2>(k, boxes, ring0);
+    dir_fluxes_c<S, C, FM, g, 3>(k, boxes, ring0);
+    __syncthreads();
+    if (g + NST < GroupCfg<G>::NGROUP && k.tid == 0) issue_group_load<G>(k, g + NST, slot);
+    dir_divergence_c<S, C, g, 0>(k);
+    dir_divergence_c<S, C, g, 1>(k);
+    dir_divergence_c<S, C, g, 2>(k);
+    dir_divergence_c<S, C, g, 3>(k);
+}
+
 template <class S>
 struct FluxGroup {
     static constexpr int value = sizeof(S) == 4 ? 4 : 1;
@@ -828,8 +895,16 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
 #pragma unroll 1
             for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 2>(k, g);
         } else if (sp.fm) {
+            if constexpr (G == 4) {
+                // the common case: narrow-range WENO5 in FP32, directions
+                // fixed at compile time
+                dir_group_c<S, C, 1, 0>(k);
+                dir_group_c<S, C, 1, 1>(k);
+                dir_group_c<S, C, 1, 2>(k);
+            } else {
 #pragma unroll 1
-            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 1>(k, g);
+                for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 1>(k, g);
+            }
         } else {
 #pragma unroll 1
             for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 0>(k, g);
