@@ -237,7 +237,7 @@ struct GroupCfg {
 // direction m of group g: G = 1 -> 1..12; G = 2 -> (1,3) (2,4) (5,7) (6,8)
 // (9,11) (10,12); G = 4 -> (1,3,2,4) (5,7,6,8) (9,11,10,12)
 template <int G>
-__host__ __device__ __forceinline__ int group_dir(int g, int m)
+__host__ __device__ constexpr int group_dir(int g, int m)
 {
     if (G == 1) return g + 1;
     if (G == 4) return 4 * g + 1 + (m >> 1) + 2 * (m & 1);
@@ -737,67 +737,70 @@ __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
     // every reader of this group has passed.
 }
 
-// Direction m of group g for four directions per group (group_dir<4>), its
-// components as constants (the D2Q13 table: e1..e4 = (1,0) (0,1) (-1,0)
-// (0,-1), e5..e8 = (1,1) (-1,1) (-1,-1) (1,-1), e9..e12 = 2 e1..2 e4).
-template <int g, int m>
-struct Dir4 {
-    static constexpr int i = 4 * g + 1 + (m >> 1) + 2 * (m & 1);
-    static constexpr int EX = m == 0 ? (g == 2 ? 2 : 1)
-                            : m == 1 ? (g == 2 ? -2 : -1)
-                            : m == 2 ? (g == 1 ? -1 : 0)
-                                     : (g == 1 ? 1 : 0);
-    static constexpr int EY = m == 0 ? (g == 1 ? 1 : 0)
-                            : m == 1 ? (g == 1 ? -1 : 0)
-                            : m == 2 ? (g == 2 ? 2 : 1)
-                                     : (g == 2 ? -2 : -1);
+// The D2Q13 velocity table as compile-time constants (c_EX, c_EY on the
+// device); DirC<G, g, m>: direction m of group g (group_dir<G>) with its
+// components.
+struct DirTable {
+    static constexpr int EX[NQ] = {0, 1, 0, -1, 0, 1, -1, -1, 1, 2, 0, -2, 0};
+    static constexpr int EY[NQ] = {0, 0, 1, 0, -1, 1, 1, -1, -1, 0, 2, 0, -2};
+};
+template <int G, int g, int m>
+struct DirC {
+    static constexpr int i = group_dir<G>(g, m);
+    static constexpr int EX = DirTable::EX[i], EY = DirTable::EY[i];
 };
 
-template <class S, class C, int FM, int g, int m>
-__device__ __forceinline__ void dir_fluxes_c(TileCtx<S, C> &k, const S *boxes, int &ring0)
+// Simple tiles with every direction fixed at compile time: the group loop
+// and the loop over a group's directions unrolled, each direction's
+// components constants (strides, signs, which faces and edge items exist).
+template <class S, class C, int FM, int G, int g, int m>
+__device__ __forceinline__ void group_fluxes_c(TileCtx<S, C> &k, const S *boxes, int &ring0)
 {
-    using D = Dir4<g, m>;
-    const int NT = k.NT;
-    constexpr int b = (g & 1) * 4 + m;
-    dir_fluxes<S, C, true, FM, D::EX, D::EY>(k, D::i, boxes + (size_t)(2 * m) * k.pstride, k.sf + (size_t)b * 4 * NT,
-                                             k.ringx + (size_t)b * 2 * k.TY, k.ringy + (size_t)b * 2 * k.TX, ring0);
-    ring0 += (D::EX ? k.TY : 0) + (D::EY ? k.TX : 0);
-    while (ring0 >= NT) ring0 -= NT;
-}
-
-template <class S, class C, int g, int m>
-__device__ __forceinline__ void dir_divergence_c(TileCtx<S, C> &k)
-{
-    using D = Dir4<g, m>;
-    constexpr int b = (g & 1) * 4 + m;
-    dir_divergence<S, C, D::EX, D::EY>(k, D::i, k.sf + (size_t)b * 4 * k.NT, k.ringx + (size_t)b * 2 * k.TY,
-                                       k.ringy + (size_t)b * 2 * k.TX);
-}
-
-// dir_group for simple tiles with the group fixed at compile time (four
-// directions per group): every direction's components are constants.
-template <class S, class C, int FM, int g>
-__device__ __forceinline__ void dir_group_c(TileCtx<S, C> &k)
-{
-    constexpr int G = 4, NST = GroupCfg<G>::NSTAGE;
-    constexpr int slot = g % NST;
-    constexpr uint32_t parity = (g / NST) & 1;
-    if (!mbar_wait_bounded(&k.bars[slot], parity, TMA_WAIT_POLLS)) {
-        *k.timed_out = 1;
-        atomicOr(k.status, STATUS_TIMEOUT);
+    if constexpr (m < G) {
+        using D = DirC<G, g, m>;
+        const int NT = k.NT;
+        constexpr int b = (g & 1) * G + m;
+        dir_fluxes<S, C, true, FM, D::EX, D::EY>(k, D::i, boxes + (size_t)(2 * m) * k.pstride,
+                                                 k.sf + (size_t)b * 4 * NT, k.ringx + (size_t)b * 2 * k.TY,
+                                                 k.ringy + (size_t)b * 2 * k.TX, ring0);
+        ring0 += (D::EX ? k.TY : 0) + (D::EY ? k.TX : 0);
+        while (ring0 >= NT) ring0 -= NT;
+        group_fluxes_c<S, C, FM, G, g, m + 1>(k, boxes, ring0);
     }
-    const S *boxes = k.stg + (size_t)slot * 2 * G * k.pstride;
-    int ring0 = 0;
-    dir_fluxes_c<S, C, FM, g, 0>(k, boxes, ring0);
-    dir_fluxes_c<S, C, FM, g, 1>(k, boxes, ring0);
-    dir_fluxes_c<S, C, FM, g, 2>(k, boxes, ring0);
-    dir_fluxes_c<S, C, FM, g, 3>(k, boxes, ring0);
-    __syncthreads();
-    if (g + NST < GroupCfg<G>::NGROUP && k.tid == 0) issue_group_load<G>(k, g + NST, slot);
-    dir_divergence_c<S, C, g, 0>(k);
-    dir_divergence_c<S, C, g, 1>(k);
-    dir_divergence_c<S, C, g, 2>(k);
-    dir_divergence_c<S, C, g, 3>(k);
+}
+
+template <class S, class C, int G, int g, int m>
+__device__ __forceinline__ void group_divergence_c(TileCtx<S, C> &k)
+{
+    if constexpr (m < G) {
+        using D = DirC<G, g, m>;
+        constexpr int b = (g & 1) * G + m;
+        dir_divergence<S, C, D::EX, D::EY>(k, D::i, k.sf + (size_t)b * 4 * k.NT, k.ringx + (size_t)b * 2 * k.TY,
+                                           k.ringy + (size_t)b * 2 * k.TX);
+        group_divergence_c<S, C, G, g, m + 1>(k);
+    }
+}
+
+// dir_group with the group fixed at compile time, then the next group
+template <class S, class C, int FM, int G, int g>
+__device__ __forceinline__ void run_groups_c(TileCtx<S, C> &k)
+{
+    if constexpr (g < GroupCfg<G>::NGROUP) {
+        constexpr int NST = GroupCfg<G>::NSTAGE;
+        constexpr int slot = g % NST;
+        constexpr uint32_t parity = (g / NST) & 1;
+        if (!mbar_wait_bounded(&k.bars[slot], parity, TMA_WAIT_POLLS)) {
+            *k.timed_out = 1;
+            atomicOr(k.status, STATUS_TIMEOUT);
+        }
+        const S *boxes = k.stg + (size_t)slot * 2 * G * k.pstride;
+        int ring0 = 0;
+        group_fluxes_c<S, C, FM, G, g, 0>(k, boxes, ring0);
+        __syncthreads();
+        if (g + NST < GroupCfg<G>::NGROUP && k.tid == 0) issue_group_load<G>(k, g + NST, slot);
+        group_divergence_c<S, C, G, g, 0>(k);
+        run_groups_c<S, C, FM, G, g + 1>(k);
+    }
 }
 
 template <class S>
@@ -890,17 +893,16 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     sD[tid] = C(0);          // direction 0 streams nothing
     sD[NQ * NT + tid] = C(0);
     if (PATH == FLUX_SIMPLE) {
-        // simple tiles: the flux scheme fixed at compile time (smaller hot code)
+        // simple tiles: the flux scheme fixed at compile time (smaller hot
+        // code); for narrow-range WENO5, the common case, in FP32 and in the
+        // FP64 final phase also every direction (the other instances lose
+        // more to their larger code than they gain)
         if (sp.fm && sizeof(S) == 4 && sp.wide) {
 #pragma unroll 1
             for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 2>(k, g);
         } else if (sp.fm) {
-            if constexpr (G == 4) {
-                // the common case: narrow-range WENO5 in FP32, directions
-                // fixed at compile time
-                dir_group_c<S, C, 1, 0>(k);
-                dir_group_c<S, C, 1, 1>(k);
-                dir_group_c<S, C, 1, 2>(k);
+            if constexpr (G == 4 || MODE == 2) {
+                run_groups_c<S, C, 1, G, 0>(k);
             } else {
 #pragma unroll 1
                 for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 1>(k, g);
