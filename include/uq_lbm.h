@@ -185,7 +185,10 @@ typedef struct lbm_batch lbm_batch;
 
 typedef struct lbm_batch_options {
     int precision;      /* LBM_PREC_F64 / LBM_PREC_F32 */
-    int tile_x, tile_y; /* 0: chosen by the autotuner's table */
+    int tile_x, tile_y; /* 0: chosen by the autotuner's table (16 x 16, the
+                           shape the stencil kernels are also compiled for;
+                           other shapes run the same kernels with the shape
+                           read at run time, bit-identical and slower) */
     int use_graph;      /* capture step sequences in CUDA graphs */
 } lbm_batch_options;
 
