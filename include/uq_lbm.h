@@ -175,6 +175,18 @@ LBM_API lbm_status lbm_mat_read_dist(const char *path, int Nx, int Ny, double *f
 /* ... and into a handle of the same case: its f, h and step count
  * (round(t / dt)) become the checkpoint's. */
 LBM_API lbm_status lbm_restore_mat(lbm_handle *h, const char *path);
+/* The Python reference's result files, ClassLBM.saveHDF5
+ * (CODE/Python/simLB/LBM.py:516-567): an HDF5 file with the datasets rho,
+ * T, ux, uy ({Nx, Ny} over [x*Ny + y]), t, gamma, R, T_ref, rho_ref, dx, dy
+ * (ndx / ndy values; scalars when 1), Nx, Ny (int64) and, when f and h are
+ * both given, f and h ({Nx, Ny, 13} over [(x*Ny + y)*13 + i]).  Doubles are
+ * little-endian IEEE.  No GPU needed. */
+LBM_API lbm_status lbm_hdf5_write_fields(const char *path, int Nx, int Ny, const double *rho, const double *ux,
+                                         const double *uy, const double *T, double t, double gamma, double R,
+                                         double T_ref, double rho_ref, const double *dx, int ndx, const double *dy,
+                                         int ndy, const double *f, const double *h);
+/* saveHDF5(all) of a handle's current state (t = step * dt). */
+LBM_API lbm_status lbm_write_hdf5(lbm_handle *h, const char *path, int with_dist);
 
 /* -------------------------------------------------------------- batches
  * Many independent samples (uneven grids, own parameters) advanced

@@ -93,3 +93,26 @@ def test_resume_from_mat_checkpoint(cuda_device, tmp_path, precision):
         assert rel_l2(fa, fb) <= 1e-6 and rel_l2(ha, hb) <= 1e-6
     a.close()
     b.close()
+
+
+def test_hdf5_output_holds_the_handle_state(tmp_path):
+    """saveHDF5(all=1) of a handle (Python reference's result file)."""
+    import hdf5_min
+    from uq_b200 import workloads as W
+
+    case = W.flat_plate(nx=24, ny=16, steps=3, tau=2e-3)  # non-uniform dy: an array
+    s = Solver(case)
+    s.step(3)
+    p = tmp_path / "step_3.hdf5"
+    s.write_hdf5(p, with_dist=True)
+    d = hdf5_min.read(p)
+    m = s.macro()
+    for k in ("rho", "ux", "uy", "T"):
+        assert np.array_equal(d[k], m[k]), k
+    f, h = s.dist()
+    assert np.array_equal(d["f"], f) and np.array_equal(d["h"], h)
+    assert d["t"] == 3 * s.dt and d["gamma"] == case["gamma"] and d["R"] == case["R"]
+    assert d["Nx"] == 24 and d["Ny"] == 16
+    assert np.ndim(d["dy"]) == 1 and len(d["dy"]) == 16 and np.ndim(d["dx"]) == 0
+    s.write_hdf5(tmp_path / "macro.hdf5")
+    assert "f" not in hdf5_min.read(tmp_path / "macro.hdf5")

@@ -11,8 +11,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = [os.path.join(HERE, "csrc", f) for f in ("lbm_kernels.cu", "lbm_engine.cu", "lbm_noalloc.cu", "lbm_server.cu", "lbm_mat.cpp")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("lbm_device.cuh", "lbm_kernels.h", "lbm_host.h", "lbm_common.h", "lbm_mat.h", "tma.cuh")] + [
+SRC = [os.path.join(HERE, "csrc", f) for f in ("lbm_kernels.cu", "lbm_engine.cu", "lbm_noalloc.cu", "lbm_server.cu", "lbm_mat.cpp", "lbm_hdf5.cpp")]
+DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("lbm_device.cuh", "lbm_kernels.h", "lbm_host.h", "lbm_common.h", "lbm_mat.h", "lbm_hdf5.h", "tma.cuh")] + [
     os.path.join(ROOT, "include", "uq_lbm.h")]
 LIB = os.path.join(HERE, "lib", "libuqlbm.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

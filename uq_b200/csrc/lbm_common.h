@@ -63,6 +63,7 @@ struct HostSample {
     int flags = 0;
     double R = 1, b = 5, K = 3, Tc = 1, c = 1, mu = 0, Pr = 1, dt = 0, tol = 0;
     double rho_ref = 1, T_ref = 1;  // completed reference state (refineInput)
+    double gamma = 1.4;
     int mu_model = 0;               // viscosity law (lbm_config::mu_model)
     double upsilon = 0, S_v = 0;
     int nsteps = 0;

@@ -8,6 +8,7 @@
 // (CODE/C++/VS2010/simLB/simLB/cpuLBM.cpp:283-450) and the step driver
 // follows runSimStep (main.cpp:32-112).
 #include "lbm_common.h"
+#include "lbm_hdf5.h"
 #include "lbm_mat.h"
 
 #include <cuda.h>
@@ -80,6 +81,7 @@ void derive_scalars(const lbm_config &c, int Nx, int Ny, double min_spacing, Sca
     s.rho_ref = rho_ref;
     s.T_ref = T_ref;
     s.b = 2 / (c.gamma - 1);
+    s.gamma = c.gamma;
     s.K = s.b - 2;
     s.Tc = c.Tc_Tref * T_ref;
     const double tau_ref = c.mu / p_ref;
@@ -146,6 +148,7 @@ HostSample derive(const lbm_config &c, const lbm_init &in)
     s.rho_ref = sc.rho_ref;
     s.T_ref = sc.T_ref;
     s.b = sc.b;
+    s.gamma = sc.gamma;
     s.K = sc.K;
     s.Tc = sc.Tc;
     s.c = sc.c;
@@ -890,6 +893,30 @@ lbm_status lbm_write_mat(lbm_handle *h, const char *path, int with_dist)
     mat_write_fields(path, s.nx, s.ny, rho.data(), ux.data(), uy.data(), p.data(), T.data(), s.step * s.dt, s.dx[0],
                      s.dy[0], with_dist ? f.data() : nullptr, with_dist ? hh.data() : nullptr,
                      with_dist ? ex.data() : nullptr, with_dist ? ey.data() : nullptr);
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_write_hdf5(lbm_handle *h, const char *path, int with_dist)
+{
+    API_BEGIN
+    if (!h || !path) throw LbmError(LBM_ERR_INVALID, "null argument");
+    lbm_batch &b = h->b;
+    const HostSample &s = b.hs[0];
+    const size_t n = (size_t)s.nx * s.ny;
+    std::vector<double> rho(n), ux(n), uy(n), T(n), p(n), f, hh;
+    b.get_macro(0, rho.data(), ux.data(), uy.data(), T.data(), p.data());
+    if (with_dist) {
+        f.resize(n * NQ);
+        hh.resize(n * NQ);
+        b.dist_io(0, f.data(), hh.data(), nullptr, nullptr);
+    }
+    // dx, dy: one value for uniform cells (as the reference's scalars)
+    const bool ux1 = std::all_of(s.dx.begin(), s.dx.end(), [&](double v) { return v == s.dx[0]; });
+    const bool uy1 = std::all_of(s.dy.begin(), s.dy.end(), [&](double v) { return v == s.dy[0]; });
+    hdf5_write_fields(path, s.nx, s.ny, rho.data(), ux.data(), uy.data(), T.data(), s.step * s.dt, s.gamma, s.R,
+                      s.T_ref, s.rho_ref, s.dx.data(), ux1 ? 1 : (int)s.dx.size(), s.dy.data(),
+                      uy1 ? 1 : (int)s.dy.size(), with_dist ? f.data() : nullptr, with_dist ? hh.data() : nullptr);
     return LBM_OK;
     API_END
 }

@@ -30,7 +30,7 @@ struct LbmError : std::runtime_error {
 struct ScalarParams {
     int rk = 1, fm = 1, flags = 0, nsteps = 0;
     double R = 1, b = 5, K = 3, Tc = 1, c = 1, mu = 0, Pr = 1, dt = 0, tol = 0;
-    double dx = 1, dy = 1, rho_ref = 1, T_ref = 1;
+    double dx = 1, dy = 1, rho_ref = 1, T_ref = 1, gamma = 1.4;
     int mu_model = 0;  // 0 constant, 1 VHS, 2 Sutherland
     double upsilon = 0, S_v = 0;
 };

@@ -134,6 +134,9 @@ SIGNATURES = {
     "lbm_write_mat": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "lbm_mat_read_dist": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _dp, _dp, _dp]),
     "lbm_restore_mat": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "lbm_hdf5_write_fields": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
+                                        C.c_double, C.c_double, C.c_double, _dp, C.c_int, _dp, C.c_int, _dp, _dp]),
+    "lbm_write_hdf5": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "lbm_step_noalloc": (C.c_int, [C.POINTER(LbmConfig), C.c_int, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_int,
                                    C.c_void_p]),
 }

@@ -91,6 +91,22 @@ def write_mat_fields(path, fields, t=0.0, dx=1.0, dy=1.0, f=None, h=None, ex=Non
                                          float(dy), *ptr), "lbm_mat_write_fields")
 
 
+def write_hdf5_fields(path, fields, t=0.0, gamma=1.4, R=1.0, T_ref=1.0, rho_ref=1.0, dx=1.0, dy=1.0, f=None,
+                      h=None):
+    """ClassLBM.saveHDF5's file (LBM.py:516-567) from host arrays: fields
+    rho, T, ux, uy as [x, y] arrays; dx, dy scalars or per-cell arrays; f, h
+    [x, y, 13] optional (both or neither)."""
+    nx, ny = fields["rho"].shape
+    arrs = [np.ascontiguousarray(fields[k], dtype=np.float64).reshape(-1) for k in ("rho", "ux", "uy", "T")]
+    dxa = np.ascontiguousarray(np.atleast_1d(dx), dtype=np.float64)
+    dya = np.ascontiguousarray(np.atleast_1d(dy), dtype=np.float64)
+    dist = [None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (f, h)]
+    ptr = [None if a is None else _d(a) for a in dist]
+    N.check(N.lib().lbm_hdf5_write_fields(str(path).encode(), nx, ny, *[_d(a) for a in arrs], float(t), float(gamma),
+                                          float(R), float(T_ref), float(rho_ref), _d(dxa), dxa.size, _d(dya),
+                                          dya.size, *ptr), "lbm_hdf5_write_fields")
+
+
 class Solver:
     """One solver instance (an ``lbm_handle``): the drop-in for cpuLBM."""
 
@@ -103,6 +119,11 @@ class Solver:
         """createMAT of the current state (rho, ux, uy, p, T, t, dx, dy; f,
         h, ex, ey with with_dist)."""
         N.check(N.lib().lbm_write_mat(self._h, str(path).encode(), 1 if with_dist else 0), "lbm_write_mat")
+
+    def write_hdf5(self, path, with_dist=False):
+        """ClassLBM.saveHDF5(all) of the current state: rho, T, ux, uy, t,
+        gamma, R, T_ref, rho_ref, dx, dy, Nx, Ny (f, h with with_dist)."""
+        N.check(N.lib().lbm_write_hdf5(self._h, str(path).encode(), 1 if with_dist else 0), "lbm_write_hdf5")
 
     def restore_mat(self, path):
         """Resume from a file write_mat(path, with_dist=True) made: f, h and
