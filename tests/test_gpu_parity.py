@@ -165,13 +165,22 @@ def test_checkpoint_roundtrip(cuda_device):
 
 def test_status_reports_nonfinite_and_equilibrium(cuda_device):
     case = W.couette(nx=16, ny=16, steps=3, seed=1)
-    s = Solver(case)
-    f, h = s.dist()
+    for prec in ("f64", "f32"):
+        s = Solver(case, prec)
+        f, h = s.dist()
+        f2 = f.copy()
+        f2[5, 7, 3] = np.nan  # host-side corruption of one value
+        s.set_dist(f2, h)
+        code, _ = s.step(1)
+        assert code == native.LBM_ERR_NONFINITE, prec
+    # in a batch only the corrupted sample is flagged (FP32 finiteness sums)
+    b = Batch([case, W.couette(nx=40, ny=24, steps=3, seed=2)], "f32")
+    f, h = b.dist(0)
     f2 = f.copy()
-    f2[5, 7, 3] = np.nan  # host-side corruption of one value
-    s.set_dist(f2, h)
-    code, _ = s.step(1)
-    assert code == native.LBM_ERR_NONFINITE
+    f2[5, 7, 3] = np.nan
+    b.set_dist(0, f2, h)
+    b.step(1)
+    assert list(b.status()) == [native.LBM_ERR_NONFINITE, native.LBM_OK]
     # an enormous velocity breaks the equilibrium mass check, as in the reference
     big = W.random_state(8, 8, seed=1, du=0.0, steps=2)
     big["velocityX"][:] = 3e4
