@@ -339,14 +339,16 @@ LBM_API lbm_status lbm_selftest_bounded_wait(int arrive);
 /* ------------------------------------------------- allocation-free step
  * No counterpart in the reference.  For callers that cannot call
  * cudaMalloc: an application that owns all device memory through its own
- * pool or arena, or code running where device allocation is not allowed
- * (for example while it records work for later replay).  It advances one
+ * pool or arena, or one whose device-memory budget is already spoken for,
+ * so that an allocation by a library it calls would fail or break its
+ * accounting.  It advances one
  * domain n_steps steps on the FP64 path with every scratch buffer taken
  * from a fixed array that the library reserves on each GPU it is loaded on
  * (about 10.7 MB, held until the process exits) -- nothing is allocated.
  *
  *   cellType  host array [Nx*Ny], the cell type (0 fluid, 1 permanent,
- *             2 solid) of each node in [x*Ny + y] order
+ *             2 solid) of each node in [x*Ny + y] order; any other value
+ *             returns LBM_ERR_INVALID before any device work
  *   d_f, d_h  device arrays [(x*Ny + y)*13 + i] (the reference's f_G, h_G
  *             layout) holding the state; updated in place
  *   stream    cudaStream_t to run on (NULL: the default stream); the call

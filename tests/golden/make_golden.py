@@ -60,7 +60,9 @@ def save(name, entries):
     print(name, len(entries), "cases")
 
 
-MAT_INPUT = "/root/reference/Items/11.04.06-BoundaryLayer-Jacobs/input.mat"
+# the reference tree: UQ_REFERENCE_ROOT, else where this container mounts it
+REF_ROOT = os.environ.get("UQ_REFERENCE_ROOT", "/root/reference")
+MAT_INPUT = os.path.join(REF_ROOT, "Items", "11.04.06-BoundaryLayer-Jacobs", "input.mat")
 
 
 def mat_input():

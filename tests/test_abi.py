@@ -90,3 +90,20 @@ def test_oversized_sample_is_rejected_before_reading_arrays():
     assert L.lbm_create(ctypes.byref(bufs.cfg), ctypes.byref(bufs.ini), 1, ctypes.byref(h)) == native.LBM_ERR_INVALID
     assert b"too large" in L.lbm_last_error()
     assert not h.value
+
+
+def test_noalloc_rejects_bad_cell_types_before_device_work():
+    """lbm_step_noalloc checks the host cellType array first (0 fluid,
+    1 permanent, 2 solid), so no GPU is needed to see the refusal."""
+    L = native.lib()
+    case = W.couette(nx=8, ny=8, steps=1)
+    from uq_b200.solver import _CaseBuffers
+
+    bufs = _CaseBuffers(case)
+    ctype = np.zeros(8 * 8, dtype=np.int32)
+    ctype[9] = 3
+    fake = ctypes.c_void_p(0x1000)  # never dereferenced: the check comes first
+    code = L.lbm_step_noalloc(ctypes.byref(bufs.cfg), 8, 8, ctype.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                              fake, fake, 1, None)
+    assert code == native.LBM_ERR_INVALID
+    assert b"cellType" in L.lbm_last_error()

@@ -21,7 +21,10 @@ from golden_util import GOLDEN, rel_max
 
 sio = pytest.importorskip("scipy.io")
 
-REF_INPUT = "/root/reference/Items/11.04.06-BoundaryLayer-Jacobs/input.mat"
+# the reference's own input file, read from the reference tree named by the
+# UQ_REFERENCE_ROOT environment variable (the test is skipped without it)
+_REF_ROOT = os.environ.get("UQ_REFERENCE_ROOT", "")
+REF_INPUT = os.path.join(_REF_ROOT, "Items", "11.04.06-BoundaryLayer-Jacobs", "input.mat") if _REF_ROOT else ""
 SCALARS = ("RKMETHOD", "FMETHOD", "CFL", "dtau", "tt_tref", "tt_time", "steps", "tol", "periodicX", "periodicY",
            "mirrorNorth", "mirrorSouth", "mirrorEast", "mirrorWest", "gamma", "R", "mu", "Pr", "dx", "dy", "Lx",
            "Ly", "rho_ref", "p_ref", "T_ref", "Tc_Tref")
@@ -106,6 +109,24 @@ def test_bad_inputs_are_rejected(tmp_path):
     assert e.value.code == N.LBM_ERR_INVALID and b"bndArray" in N.lib().lbm_last_error()
 
 
+def test_negative_dimensions_are_rejected(tmp_path):
+    """A variable whose stored dimensions are negative is refused, not
+    wrapped into a huge (or, multiplied, a small) element count."""
+    import struct
+
+    case = W.couette(nx=8, ny=8, steps=1)
+    p = tmp_path / "negdims.mat"
+    sio.savemat(str(p), _as_mat_vars(case, False), do_compression=False)
+    raw = bytearray(p.read_bytes())
+    at = raw.index(b"bndArray")  # name data; its 8-byte tag and the 2-int32 dims data come before it
+    assert struct.unpack_from("<ii", raw, at - 16) == (8, 8)
+    struct.pack_into("<ii", raw, at - 16, -1, -1)
+    p.write_bytes(bytes(raw))
+    with pytest.raises(N.LbmError) as e:
+        mat_case(p)
+    assert e.value.code == N.LBM_ERR_INVALID and b"negative" in N.lib().lbm_last_error()
+
+
 def _fixture_case():
     z = np.load(os.path.join(GOLDEN, "mat_boundary_layer.npz"))
     case = {k[5:]: z[k] for k in z.files if k.startswith("case_")}
@@ -116,7 +137,8 @@ def _fixture_case():
     return case, {k[4:]: z[k] for k in z.files if k.startswith("out_")}
 
 
-@pytest.mark.skipif(not os.path.exists(REF_INPUT), reason="reference tree not present")
+@pytest.mark.skipif(not REF_INPUT or not os.path.exists(REF_INPUT),
+                    reason="set UQ_REFERENCE_ROOT to the reference tree to read its input.mat")
 def test_reference_input_file():
     _case_equal(mat_case(REF_INPUT), _fixture_case()[0])
 

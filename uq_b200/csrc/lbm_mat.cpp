@@ -133,13 +133,19 @@ bool parse_matrix(const Reader &r, const uint8_t *q, size_t len, std::string &na
     const uint32_t cls = sub.u32((size_t)(flags.data - q)) & 0xff;
     if (!read_element(sub, flags.next, dims) || dims.type != miINT32) return false;
     v.dims.clear();
-    for (size_t i = 0; i + 4 <= dims.len; i += 4) v.dims.push_back((size_t)load_as<int32_t>(dims.data + i, r.swap));
+    for (size_t i = 0; i + 4 <= dims.len; i += 4) {
+        const int32_t d = load_as<int32_t>(dims.data + i, r.swap);
+        if (d < 0) throw LbmError(LBM_ERR_INVALID, "MAT variable with a negative dimension");
+        v.dims.push_back((size_t)d);
+    }
     if (!read_element(sub, dims.next, nm) || (nm.type != miINT8 && nm.type != miUTF8)) return false;
     name.assign(reinterpret_cast<const char *>(nm.data), nm.len);
     if (cls < mxDOUBLE || cls > mxUINT64 || cls == mxSPARSE || cls == mxCHAR) return false;
     if (!read_element(sub, nm.next, real)) return false;
     size_t count = 1;
-    for (size_t d : v.dims) count *= d;
+    for (size_t d : v.dims)
+        if (__builtin_mul_overflow(count, d, &count))
+            throw LbmError(LBM_ERR_INVALID, "MAT variable whose element count overflows");
     if (!numeric_to_double(real.type, real.data, real.len, r.swap, v.data) || v.data.size() != count) return false;
     return true;
 }

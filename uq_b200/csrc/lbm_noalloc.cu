@@ -1,12 +1,12 @@
 // lbm_step_noalloc: the FP64 step of one small domain with no device
 // allocation.  Some callers cannot call cudaMalloc: a host application that
-// owns all device memory through its own pool or arena, or code that runs
-// while device allocation is forbidden (inside a region it is capturing for
-// replay, or on a device whose memory budget is already spoken for).  For
-// them the stage buffers, wall factors, node flags, tile list and TMA
-// descriptors that lbm_create would cudaMalloc live in one file-scope
-// device array of fixed size instead, and the caller passes only its own
-// f and h arrays (device memory it already owns).
+// owns all device memory through its own pool or arena, or one whose
+// device-memory budget is already spoken for, so that a library's own
+// allocation would fail or break its accounting.  For them the stage
+// buffers, wall factors, node flags, tile list and TMA descriptors that
+// lbm_create would cudaMalloc live in one file-scope device array of fixed
+// size instead, and the caller passes only its own f and h arrays (device
+// memory it already owns).
 //
 // The array is reserved on every GPU that loads this library, until the
 // process exits.  Every call shares it and overwrites what the last call
@@ -199,6 +199,10 @@ static lbm_status step_noalloc(const lbm_config *cfg, int Nx, int Ny, const int 
     if (cfg->dx_array || cfg->dy_array)
         throw LbmError(LBM_ERR_INVALID, "lbm_step_noalloc supports uniform cells only");
     if (Nx < 3 || Ny < 3) throw LbmError(LBM_ERR_INVALID, "Nx and Ny must be at least 3");
+    // the node flags keep the cell type in two bits next to the stencil
+    // bits: a value outside 0..2 would mark interior nodes as boundaries
+    for (long long k = 0; k < (long long)Nx * Ny; ++k)
+        if (cellType[k] < 0 || cellType[k] > 2) throw LbmError(LBM_ERR_INVALID, "cellType must be 0, 1 or 2");
     const int pitch = (Nx + 31) / 32 * 32;
     if ((long long)Ny * pitch > NA_MAX_NODES || Nx > NA_MAX_LINE || Ny > NA_MAX_LINE)
         throw LbmError(LBM_ERR_INVALID, "domain exceeds lbm_step_noalloc's fixed scratch: Ny * roundup(Nx, 32) must be <= " +
