@@ -47,6 +47,10 @@ def parse():
                     help="Poisson arrival window of the serving run (0: skip it)")
     ap.add_argument("--no-probes", action="store_true",
                     help="only the timed ensemble run: no accuracy, plain-FP64, serving or CPU runs (profiling)")
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="steps of the FP32-vs-FP64 ensemble comparison (the configuration's 1000; 0: skip it)")
+    ap.add_argument("--long", action="store_true",
+                    help="also run the flat-plate batch for its configured 20000 steps (about 3 minutes)")
     return ap.parse_args()
 
 
@@ -106,47 +110,81 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_reference_arm(n_procs, steps_per_proc, samples, seed_offset=0):
-    """Time the reference C++ solver (or, if it is absent, the FP64 C
-    restatement) on independent ensemble samples, one process per core."""
+# steps each reference process runs per bench step, by grid side: about
+# 2.6e5 lattice updates (a few seconds of one core) for every side
+REF_SIDE_STEPS = {64: 64, 128: 16, 256: 4, 512: 1}
+
+
+def cpu_reference_arm(samples, n_procs):
+    """The reference C++ solver (oracle/_ref, built from the reference's
+    unmodified sources; else the FP64 C restatement) on the ensemble's own
+    mix of grid sides.
+
+    The reference has no threading, so n_procs independent processes run at
+    once, one ensemble sample each, cycling through the sides 64, 128, 256,
+    512 (REF_SIDE_STEPS steps each).  Each process reports the seconds of its
+    own step loop, giving the cost of a lattice update per side with every
+    core busy.  The ensemble's CPU throughput is then n_procs x its nodes
+    over one pass of it at those per-side costs:
+        MLUPS = n_procs * sum_s N_s / sum_s (N_s * t_LU(s)),
+    N_s the ensemble's nodes on grids of side s."""
     from oracle import refrun
     from uq_b200 import workloads as W
 
-    picks = [d for d in samples if d["nx"] == 64][: max(n_procs, 1)]
-    while len(picks) < n_procs:
-        picks.append(dict(picks[-1], seed=picks[-1]["seed"] + 1))
-    lu = 0
+    sides = sorted(REF_SIDE_STEPS)
+    by_side = {sd: [d for d in samples if d["nx"] == sd] for sd in sides}
+    nodes_by_side = {sd: sum(d["nx"] * d["ny"] for d in by_side[sd]) for sd in sides}
+    total_nodes = sum(nodes_by_side.values())
+    present = [sd for sd in sides if by_side[sd]]
+    t_lu = {}
     if refrun.available():
         kind = "reference"
+        picks = []
+        for j in range(max(n_procs, len(present))):
+            sd = present[j % len(present)]
+            lst = by_side[sd]
+            picks.append((sd, lst[(j // len(present)) % len(lst)]))
         tmp = tempfile.mkdtemp(prefix="refarm_")
-        procs = []
-        for k, d in enumerate(picks):
+        procs, work = [], []
+        for k, (sd, d) in enumerate(picks):
             wd = os.path.join(tmp, "p%d" % k)
             os.makedirs(wd)
-            case = W.ensemble_case(dict(d, steps=steps_per_proc))
-            refrun.write_lbmv(os.path.join(wd, "case.lbmv"), refrun.case_to_vars(case))
-            lu += case["bnd"].size * steps_per_proc
+            steps = REF_SIDE_STEPS[sd]
+            refrun.write_lbmv(os.path.join(wd, "case.lbmv"), refrun.case_to_vars(W.ensemble_case(dict(d, steps=steps))))
+            work.append((sd, wd, d["nx"] * d["ny"] * steps))
         t0 = time.perf_counter()
-        for k in range(len(picks)):
-            wd = os.path.join(tmp, "p%d" % k)
-            procs.append(subprocess.Popen([refrun.REF_BIN, "case.lbmv", "out.lbmv", str(steps_per_proc)], cwd=wd,
+        for sd, wd, _ in work:
+            procs.append(subprocess.Popen([refrun.REF_BIN, "case.lbmv", "out.lbmv", str(REF_SIDE_STEPS[sd])], cwd=wd,
                                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
         for p in procs:
             p.wait()
         wall = time.perf_counter() - t0
+        per = {sd: [] for sd in sides}
+        for sd, wd, lu in work:
+            secs = float(refrun.read_lbmv(os.path.join(wd, "out.lbmv"))["scalars"][7])
+            per[sd].append(secs / lu)
         subprocess.run(["rm", "-rf", tmp])
+        cores = len(picks)
+        t_lu = {sd: float(np.mean(v)) for sd, v in per.items() if v}
     else:
         kind = "port"
         from oracle import oracle as O
 
-        case = W.ensemble_case(dict(picks[0], steps=steps_per_proc))
-        o = O.Oracle(case)
         t0 = time.perf_counter()
-        o.step(steps_per_proc)
+        for sd in present:
+            d = by_side[sd][0]
+            steps = max(1, REF_SIDE_STEPS[sd] // 8)
+            o = O.Oracle(W.ensemble_case(dict(d, steps=steps)))
+            t1 = time.perf_counter()
+            o.step(steps)
+            t_lu[sd] = (time.perf_counter() - t1) / (d["nx"] * d["ny"] * steps)
         wall = time.perf_counter() - t0
-        lu = case["bnd"].size * steps_per_proc
-        n_procs = 1
-    return lu / wall / 1e6, n_procs, kind, wall
+        cores = 1
+    pass_s = sum(nodes_by_side[sd] * t_lu[sd] for sd in present)
+    mlups = cores * total_nodes / pass_s / 1e6
+    detail = {"us_per_lu_by_side": {str(sd): 1e6 * t_lu[sd] for sd in present},
+              "node_share_by_side": {str(sd): nodes_by_side[sd] / total_nodes for sd in present}}
+    return mlups, cores, kind, wall, detail
 
 
 def run_reference_impl(args, rank, world):
@@ -156,25 +194,27 @@ def run_reference_impl(args, rank, world):
 
     samples = W.uq_ensemble(n=args.samples, seed=args.seed)
     ncores = os.cpu_count() or 1
-    per = 20
     for _ in range(args.warmup):
-        cpu_reference_arm(ncores, 2, samples)
+        cpu_reference_arm(samples, ncores)
     vals, walls = [], []
-    kind = "reference"
+    kind, detail = "reference", {}
     for _ in range(args.steps):
-        v, cores, kind, wall = cpu_reference_arm(ncores, per, samples)
+        v, cores, kind, wall, detail = cpu_reference_arm(samples, ncores)
         vals.append(v)
         walls.append(wall)
     value = float(np.mean(vals))
+    sample = ("per bench step %d concurrent reference processes, one ensemble sample each, cycling through the "
+              "sides 64/128/256/512 (%s steps); per-side cost per lattice update weighted by the ensemble's node "
+              "share" % (cores, "/".join(str(REF_SIDE_STEPS[s]) for s in sorted(REF_SIDE_STEPS))))
     out = {
         "metric": "batched f+h MLUPS (UQ ensemble, WENO5 RK3)", "value": value, "unit": "MLUPS",
         "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * float(np.mean(walls)), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "samples": args.samples, "reference_sample":
-                   "%d independent reference processes, each one 64x64 ensemble sample for %d steps" % (ncores, per)},
-        "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": ncores, "kind": kind,
-                         "sample": "%d processes x 64x64 Couette sample x %d steps per bench step" % (ncores, per)},
+        "config": {"workload": WORKLOAD, "samples_per_gpu": args.samples, "sides": [64, 128, 256, 512],
+                   "seed": args.seed, "reference_sample": sample},
+        "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": cores, "kind": kind, "sample": sample,
+                         **detail},
         "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -196,62 +236,113 @@ def field_errors(m, r):
     return out
 
 
-def accuracy_probe(samples, steps=10):
-    """Mixed path vs the FP64 path on every sample of the ensemble after
-    `steps` steps: per-sample relative L2 of rho, |u|, T; the worst sample,
-    the median and the count within 1e-5."""
+def _timed_steps(b, n):
+    """Device time (ms) of n steps of a batch, CUDA events on its stream."""
+    import torch
+
+    st = torch.cuda.ExternalStream(b.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    b.step(n)
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def ulp_perturbed(case, seed=77):
+    """The same case with every interior node's density moved by one unit in
+    the last place, up or down (seeded): the inputs of a second FP64 run that
+    differs from the first only by rounding."""
+    rng = np.random.default_rng(seed)
+    d = np.asarray(case["density"], dtype=np.float64).copy()
+    d[2:] = np.nextafter(d[2:], rng.choice([-np.inf, np.inf], size=d.size - 2))
+    return dict(case, density=d)
+
+
+def accuracy_probe(samples, steps=1000):
+    """The mixed path against the FP64 path on every sample of the ensemble
+    after `steps` steps (the configuration's full length), with the FP64
+    floor beside it.
+
+    Three batches run the ensemble: FP64, FP64 with every interior density
+    moved by 1 ulp (ulp_perturbed), and FP32.  Reported per precision: how
+    many samples finished with status 0; over the samples all three finished:
+    the relative L2 of rho, |u|, T of FP32 against FP64 (max, median, count
+    within 1e-5), the same for the perturbed FP64 run (the floor: how far two
+    FP64 runs drift apart from rounding alone), and FP32's error in units of
+    that floor.  The FP64 batch's time gives the batched FP64 MLUPS of the
+    same ensemble and step count."""
     from uq_b200 import workloads as W
     from uq_b200.solver import Batch
 
     cases = [W.ensemble_case(d) for d in samples]
-    b32 = Batch(cases, "f32")
-    b64 = Batch(cases, "f64")
-    b32.step(steps)
-    b64.step(steps)
-    per = {"rho": [], "u": [], "T": []}
-    for k in range(len(cases)):
-        e = field_errors(b32.macro(k), b64.macro(k))
-        for name in per:
-            per[name].append(e[name][0])
-    b32.close()
-    b64.close()
-    worst = {k: float(np.max(v)) for k, v in per.items()}
-    med = {k: float(np.median(v)) for k, v in per.items()}
-    ok = int(sum(all(per[k][j] <= 1e-5 for k in per) for j in range(len(cases))))
-    return {"steps": steps, "samples": len(cases), "l2_rel_max": worst, "l2_rel_median": med,
-            "samples_within_1e-5": ok}
+
+    def run(cs, prec):
+        b = Batch(cs, prec)
+        ms = _timed_steps(b, steps)
+        mlups = b.nodes * steps / (ms * 1e3)
+        st = b.status()
+        macros = [b.macro(k) for k in range(len(cs))]
+        b.close()
+        return macros, st, mlups
+
+    m64, st64, mlups64 = run(cases, "f64")
+    mp, stp, _ = run([ulp_perturbed(c) for c in cases], "f64")
+    floor = [field_errors(mp[k], m64[k]) for k in range(len(cases))]
+    del mp
+    m32, st32, mlups32 = run(cases, "f32")
+    err = [field_errors(m32[k], m64[k]) for k in range(len(cases))]
+    del m32, m64
+    ok = [k for k in range(len(cases)) if st64[k] == 0 and stp[k] == 0 and st32[k] == 0]
+    names = ("rho", "u", "T")
+
+    def summary(e):
+        v = {n: [e[k][n][0] for k in ok] for n in names}
+        return ({n: float(np.max(v[n])) if ok else None for n in names},
+                {n: float(np.median(v[n])) if ok else None for n in names})
+
+    emax, emed = summary(err)
+    fmax, fmed = summary(floor)
+    ratio = [max(err[k][n][0] / max(floor[k][n][0], 1e-300) for n in names) for k in ok]
+    sides = sorted({d["nx"] for d in samples})
+    return {
+        "steps": steps, "samples": len(cases),
+        "status_ok": {"f32": int((st32 == 0).sum()), "f64": int((st64 == 0).sum()),
+                      "f64_ulp_perturbed": int((stp == 0).sum())},
+        "failed_by_side": {str(sd): {"f32": int(sum(1 for k, d in enumerate(samples) if d["nx"] == sd and st32[k])),
+                                     "f64": int(sum(1 for k, d in enumerate(samples) if d["nx"] == sd and st64[k]))}
+                           for sd in sides},
+        "failed_same_samples": bool(np.array_equal(st32 != 0, st64 != 0)),
+        "compared_samples": len(ok),
+        "l2_rel_max": emax, "l2_rel_median": emed,
+        "samples_within_1e-5": int(sum(all(err[k][n][0] <= 1e-5 for n in names) for k in ok)),
+        "fp64_floor_l2_rel_max": fmax, "fp64_floor_l2_rel_median": fmed,
+        "f32_over_floor": {"max": float(np.max(ratio)) if ratio else None,
+                           "median": float(np.median(ratio)) if ratio else None},
+        "batched_fp64_mlups": mlups64, "batched_fp32_mlups_untimed_steps": mlups32,
+    }
 
 
-def config_probes(seed=99):
-    """The other full-size workloads, bounded.
+def config_probes(seed=99, plate_steps=50):
+    """The other full-size workloads.
 
     Riemann 2048 x 2048 (Lax-Liu 3, NND, RK1 -- the reference has no RK2 --,
     tau 1e-3, 500 steps): FP32 and FP64 timed on the device, then the FP32
     fields against the FP64 ones.  Flat plate, 16 samples of 2048 x 512 on
     the y-stretched grid with Ma ~ U(1.5, 2.5), tau ~ U(5e-4, 2e-3) (WENO5,
-    RK3): FP32 timed over 50 steps (of the configuration's 20000), and FP32
-    against FP64 after 10 steps."""
-    import torch
-
+    RK3): FP32 timed over plate_steps steps (the configuration's length is
+    20000; --long runs all of them) with the status of every sample after
+    them, and FP32 against FP64 after 10 steps."""
     from uq_b200 import workloads as W
     from uq_b200.solver import Batch
-
-    def timed(b, n):
-        st = torch.cuda.ExternalStream(b.stream)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(st)
-        b.step(n)
-        e1.record(st)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
 
     out = {}
     case = W.riemann(nx=2048, ny=2048, steps=500)
     res = {}
     for prec in ("f32", "f64"):
         b = Batch([case], prec)
-        ms = timed(b, 500)
+        ms = _timed_steps(b, 500)
         res[prec] = (b.nodes * 500 / (ms * 1e3), int(b.status()[0]), b.macro(0))
         b.close()
     err = field_errors(res["f32"][2], res["f64"][2])
@@ -263,10 +354,9 @@ def config_probes(seed=99):
     draws = [(float(rng.uniform(1.5, 2.5)), float(rng.uniform(5e-4, 2e-3))) for _ in range(16)]
     plates = [W.flat_plate(mach=m, tau=t, steps=20000) for m, t in draws]
     b = Batch(plates, "f32")
-    b.step(2)
-    ms = timed(b, 50)
-    mlups = b.nodes * 50 / (ms * 1e3)
-    st50 = b.status()
+    ms = _timed_steps(b, plate_steps)
+    mlups = b.nodes * plate_steps / (ms * 1e3)
+    st_end = b.status()
     b.close()
     b32, b64 = Batch(plates, "f32"), Batch(plates, "f64")
     b32.step(10)
@@ -279,7 +369,7 @@ def config_probes(seed=99):
     b32.close()
     b64.close()
     out["flat_plate_16x2048x512_weno5_rk3"] = {
-        "mlups_f32": mlups, "steps_timed": 50, "status_ok_after_52_steps": int((st50 == 0).sum()),
+        "mlups_f32": mlups, "steps_timed": plate_steps, "status_ok_after_timed_steps": int((st_end == 0).sum()),
         "f32_vs_f64_l2_max_10_steps": worst}
     return out
 
@@ -531,6 +621,14 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = measured_peaks()
     b_alg = B_ALG_F32 if args.precision == "f32" else B_ALG_F64
     achieved = b_alg * nodes / (phases[dom] * 1e-3) / 1e9
+    # bytes a phase must move per node, state-sized buffers read or written
+    # once (26 values each): pointwise reads the state and writes buffer 2;
+    # stencil phase 1 reads buffer 2 and the state, writes buffer 3 and the
+    # state; stencil phase 2 reads buffer 3 and the state, writes the state
+    es = 4 if args.precision == "f32" else 8
+    phase_bytes = {"pointwise": 52 * es, "stencil1": 104 * es, "stencil2": 78 * es}
+    phase_frac = {k: phase_bytes[k] * nodes / (phases[names.index(k)] * 1e-3) / 1e9 / peak
+                  for k in phase_bytes if phases[names.index(k)] > 0}
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic_per_node.json")
     if os.path.exists(tp):
@@ -574,9 +672,10 @@ def run_ours(args, rank, world, local_rank):
 
     extra = {}
     if rank == 0 and not args.no_probes:
-        extra["accuracy_vs_fp64"] = accuracy_probe(samples)
+        if args.accuracy_steps > 0:
+            extra["accuracy_vs_fp64"] = accuracy_probe(samples, args.accuracy_steps)
         try:
-            extra["configs"] = config_probes()
+            extra["configs"] = config_probes(plate_steps=20000 if args.long else 50)
         except Exception as exc:  # reported, not fatal
             extra["configs"] = {"error": repr(exc)}
         try:
@@ -585,9 +684,12 @@ def run_ours(args, rank, world, local_rank):
             extra["plain_fp64_mlups_32_samples"] = "error: %s" % exc
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.no_probes:
-        v, cores, kind, wall = cpu_reference_arm(os.cpu_count() or 1, 40, samples)
+        v, cores, kind, wall, detail = cpu_reference_arm(samples, os.cpu_count() or 1)
         cpu = {"value": v, "unit": "MLUPS", "cores": cores, "kind": kind,
-               "sample": "%d processes, each one 64x64 ensemble sample x 40 steps (%.1f s wall)" % (cores, wall)}
+               "sample": "%d concurrent reference processes, one ensemble sample each, cycling through the sides "
+                         "64/128/256/512 (%s steps), per-side cost weighted by the ensemble's node share (%.1f s "
+                         "wall)" % (cores, "/".join(str(REF_SIDE_STEPS[x]) for x in sorted(REF_SIDE_STEPS)), wall),
+               **detail}
 
     launches = b.launches_per_step(False) * args.steps
     b.close()
@@ -613,7 +715,10 @@ def run_ours(args, rank, world, local_rank):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": "k_flux " + names[dom],
                          "peak_kind": peak_kind, "alg_bytes_per_lu": b_alg,
-                         "phase_ms": dict(zip(names, [float(x) for x in phases]))},
+                         "frac_whole_step": b_alg * nodes / (ms_per_step * 1e-3) / 1e9 / peak,
+                         "phase_ms": dict(zip(names, [float(x) for x in phases])),
+                         "phase_compulsory_bytes_per_node": phase_bytes,
+                         "phase_frac_of_peak_at_compulsory_bytes": phase_frac},
             "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": h2d / args.steps,
                     "d2h_bytes_per_step": d2h / args.steps,
                     "what": "per solve: pinned host fields -> lbm_batch_set_macro, K steps, lbm_batch_get_macro"},

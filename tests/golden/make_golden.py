@@ -9,6 +9,9 @@ checksum of that input to catch builder drift.
 
     python tests/golden/make_golden.py          # regenerate all fixtures
     python tests/golden/make_golden.py mat      # only the MAT-input fixture
+    python tests/golden/make_golden.py chaos    # only the 1-ulp perturbation fixture
+    python tests/golden/make_golden.py riemann  # only the Riemann 256^2 fixture
+    python tests/golden/make_golden.py ensemble # only the ensemble's 64^2 status fixture
 
 Needs the reference tree (only in the development container); the fixtures
 themselves are committed and need nothing at test time.
@@ -93,11 +96,146 @@ def mat_input():
     print("mat_boundary_layer.npz", case["bnd"].shape, "steps", r["step"])
 
 
+CHAOS_STEPS = (10, 50, 200, 2000)
+
+
+def _ref_fields(args):
+    """One reference run (a picklable task for the process pool)."""
+    case, steps = args
+    r = refrun.run_reference(case, max_steps=steps)
+    return {k: r[k] for k in ("rho", "ux", "uy", "T")}
+
+
+def _l2_errors(a, b):
+    """Relative L2 of rho, the u vector and T over all nodes: a against b."""
+    d_u = np.sqrt((a["ux"] - b["ux"]) ** 2 + (a["uy"] - b["uy"]) ** 2)
+    return [float(np.linalg.norm(a["rho"] - b["rho"]) / np.linalg.norm(b["rho"])),
+            float(np.linalg.norm(d_u) / np.linalg.norm(np.hypot(b["ux"], b["uy"]))),
+            float(np.linalg.norm(a["T"] - b["T"]) / np.linalg.norm(b["T"]))]
+
+
+def chaos():
+    """How far two FP64 runs of the Couette workload (64 x 128, WENO5, RK3)
+    drift apart when their inputs differ by one unit in the last place.
+
+    The reference runs the workload four times: as built, with one interior
+    node's density raised by 1 ulp, with every interior node's density
+    moved by 1 ulp up or down (seeded signs), and with every interior
+    density moved by one single-precision ulp (relative 2^-24, the same
+    signs).  The fixture keeps the
+    unperturbed fields at 10, 50 and 200 steps (2000 steps are in
+    couette_64x128_2000.npz) and the relative L2 distance of rho, u, T of
+    each perturbed run from it at 10, 50, 200 and 2000 steps: the spread
+    that rounding alone produces, against which other FP64 and FP32
+    implementations are judged."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    kw = dict(nx=64, ny=128, steps=2000, seed=0)
+    base = W.build("couette", **kw)
+    one = W.build("couette", **kw)
+    k_one = 2 + 64 * 63 + 17  # an interior node's property id: x = 32, y = 18 (ids 2 + x*(Ny-2) + y-1)
+    one["density"] = one["density"].copy()
+    one["density"][k_one] = np.nextafter(one["density"][k_one], np.inf)
+    allp = W.build("couette", **kw)
+    rng = np.random.default_rng(77)
+    d = allp["density"].copy()
+    sgn = rng.choice([-np.inf, np.inf], size=d.size - 2)
+    d[2:] = np.nextafter(d[2:], sgn)
+    allp["density"] = d
+    # every interior density moved by one FP32 ulp (relative 2^-24, seeded
+    # signs): the size of a rounding to single precision
+    f32p = W.build("couette", **kw)
+    d = f32p["density"].copy()
+    d[2:] = d[2:] * (1.0 + np.sign(sgn) * 2.0 ** -24)
+    f32p["density"] = d
+    variants = [base, one, allp, f32p]
+    tasks = [(c, s) for c in variants for s in CHAOS_STEPS]
+    with cf.ProcessPoolExecutor(max_workers=min(len(tasks), os.cpu_count() or 1),
+                                mp_context=mp.get_context("spawn")) as ex:
+        res = list(ex.map(_ref_fields, tasks))
+    n = len(CHAOS_STEPS)
+    ref = res[:n]
+    arrays = {"steps": np.array(CHAOS_STEPS), "digest": np.array(case_digest(base)),
+              "kwargs": np.array(json.dumps(kw)), "one_node_id": np.array(k_one),
+              "perturb_seed": np.array(77)}
+    arrays["err_one_node"] = np.array([_l2_errors(res[n + j], ref[j]) for j in range(n)])
+    arrays["err_all_nodes"] = np.array([_l2_errors(res[2 * n + j], ref[j]) for j in range(n)])
+    arrays["err_all_nodes_f32ulp"] = np.array([_l2_errors(res[3 * n + j], ref[j]) for j in range(n)])
+    for j, s in enumerate(CHAOS_STEPS[:-1]):
+        for k in ("rho", "ux", "uy", "T"):
+            arrays["ref%d_%s" % (s, k)] = ref[j][k]
+    g = np.load(os.path.join(OUT, "couette_64x128_2000.npz"))
+    for k in ("rho", "ux", "uy", "T"):
+        assert np.array_equal(g["c0_" + k], ref[-1][k]), k  # the committed 2000-step run, bit for bit
+    np.savez_compressed(os.path.join(OUT, "couette_chaos.npz"), **arrays)
+    print("couette_chaos.npz: L2 (rho, u, T) one node", arrays["err_one_node"].tolist())
+    print("couette_chaos.npz: L2 (rho, u, T) all nodes", arrays["err_all_nodes"].tolist())
+    print("couette_chaos.npz: L2 (rho, u, T) all nodes, FP32 ulp", arrays["err_all_nodes_f32ulp"].tolist())
+
+
+def riemann_floor():
+    """The Riemann workload on a reduced 256 x 256 grid (Lax-Liu 3, NND,
+    RK1, tau 1e-3, CFL 0.2, 500 steps): the reference's FP64 fields after
+    500 steps, against which the GPU's FP64 and FP32 paths are measured."""
+    kw = dict(nx=256, ny=256, steps=500)
+    case = W.build("riemann", **kw)
+    r = refrun.run_reference(case, max_steps=500)
+    arrays = {"digest": np.array(case_digest(case)), "kwargs": np.array(json.dumps(kw)),
+              "step": np.array(r["step"])}
+    for k in ("rho", "ux", "uy", "T"):
+        arrays[k] = r[k]
+    np.savez_compressed(os.path.join(OUT, "riemann256_500.npz"), **arrays)
+    print("riemann256_500.npz steps", r["step"])
+
+
+def _ref_status(args):
+    """Reference run of one ensemble sample to `steps` steps: (stop flag,
+    steps done, all fields finite)."""
+    sample, steps = args
+    r = refrun.run_reference(W.ensemble_case(sample), max_steps=steps)
+    finite = all(np.all(np.isfinite(r[k])) for k in ("rho", "ux", "uy", "T"))
+    return int(r["stop"]), int(r["step"]), bool(finite)
+
+
+def ensemble_status(side=64, steps=1000, seed=1234, n=512):
+    """The UQ ensemble's samples of the given side (512 Couette samples,
+    u_w ~ U(0.05, 0.2), tau ~ U(0.02, 0.1), Pr ~ U(0.6, 1.0), WENO5, RK3):
+    what the reference's driver reports after `steps` steps for each --
+    stop (1: runOne's hasFailed, the equilibrium check) and the step it
+    stopped at."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    samples = W.uq_ensemble(n=n, seed=seed)
+    picks = [(k, d) for k, d in enumerate(samples) if d["nx"] == side]
+    with cf.ProcessPoolExecutor(max_workers=os.cpu_count() or 1, mp_context=mp.get_context("spawn")) as ex:
+        res = list(ex.map(_ref_status, [(d, steps) for _, d in picks]))
+    arrays = {"index": np.array([k for k, _ in picks]), "side": np.array(side), "steps": np.array(steps),
+              "seed": np.array(seed), "n": np.array(n),
+              "u_w": np.array([d["u_w"] for _, d in picks]), "tau": np.array([d["tau"] for _, d in picks]),
+              "Pr": np.array([d["Pr"] for _, d in picks]),
+              "stop": np.array([r[0] for r in res]), "step": np.array([r[1] for r in res]),
+              "finite": np.array([r[2] for r in res])}
+    np.savez_compressed(os.path.join(OUT, "ensemble%d_status.npz" % side), **arrays)
+    print("ensemble%d_status.npz: %d samples, %d stopped by the equilibrium check" %
+          (side, len(picks), int((arrays["stop"] == 1).sum())))
+
+
 def main():
     if not refrun.available():
         sys.exit("reference binary missing: make -C oracle")
     if sys.argv[1:] == ["mat"]:
         mat_input()
+        return
+    if sys.argv[1:] == ["chaos"]:
+        chaos()
+        return
+    if sys.argv[1:] == ["riemann"]:
+        riemann_floor()
+        return
+    if sys.argv[1:] == ["ensemble"]:
+        ensemble_status()
         return
 
     # (i) two steps from seeded random states: every BC family x flux x stepper
@@ -144,6 +282,9 @@ def main():
          [run("couette", dict(nx=64, ny=128, steps=2000, seed=0), keep=("rho", "ux", "uy", "T"))])
 
     mat_input()
+    chaos()
+    riemann_floor()
+    ensemble_status()
 
 
 if __name__ == "__main__":

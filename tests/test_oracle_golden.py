@@ -120,3 +120,73 @@ def test_couette_full_2000_steps():
     assert abs(mass - gmass) / gmass < 1e-11
     assert abs(energy - genergy) / genergy < 1e-3
     assert abs(Tm - gTm) / gTm < 1e-3
+
+
+def _chaos():
+    import json
+    import os
+
+    from golden_util import GOLDEN, case_digest
+    from uq_b200 import workloads as W
+
+    z = np.load(os.path.join(GOLDEN, "couette_chaos.npz"))
+    case = W.build("couette", **json.loads(str(z["kwargs"])))
+    assert case_digest(case) == str(z["digest"])
+    return case, [int(s) for s in z["steps"]], z
+
+
+def _l2_errors(m, r):
+    du = np.sqrt((m["ux"] - r["ux"]) ** 2 + (m["uy"] - r["uy"]) ** 2)
+    return np.array([rel_l2(m["rho"], r["rho"]), float(np.linalg.norm(du) / np.linalg.norm(np.hypot(r["ux"], r["uy"]))),
+                     rel_l2(m["T"], r["T"])])
+
+
+def test_reference_rounding_spread_grows_then_saturates():
+    """The fixture's own record: a 1-ulp input change grows by orders of
+    magnitude over 50 steps and saturates near the fluctuation scale."""
+    _, steps, z = _chaos()
+    for key in ("err_one_node", "err_all_nodes", "err_all_nodes_f32ulp"):
+        e = z[key]
+        assert e.shape == (len(steps), 3)
+        assert np.all(e[2] > 1e3 * e[0]) or key == "err_all_nodes_f32ulp"
+        assert np.all(e[-1] > 1e-4) and np.all(e[-1] < 1.0)
+
+
+@pytest.mark.parametrize("upto", [200, pytest.param(2000, marks=pytest.mark.slow)])
+def test_oracle_within_the_references_rounding_spread(upto):
+    """A second FP64 implementation (the C restatement, its own operation
+    order) stays within 10x the reference's 1-ulp spread at every checkpoint
+    (measured: within 1.5x)."""
+    case, steps, z = _chaos()
+    o = O.Oracle(case)
+    done = 0
+    for j, n in enumerate(steps):
+        if n > upto:
+            break
+        o.step(n - done)
+        done = n
+        if n < 2000:
+            ref = {k: z["ref%d_%s" % (n, k)] for k in ("rho", "ux", "uy", "T")}
+        else:
+            [(_, _, ref)] = load("couette_64x128_2000.npz")
+        e = _l2_errors(o.macro(), ref)
+        spread = np.maximum(z["err_one_node"][j], z["err_all_nodes"][j])
+        assert np.all(e <= 10.0 * spread), (n, e, spread)
+
+
+@pytest.mark.slow
+def test_oracle_riemann256_500_steps():
+    import json
+    import os
+
+    from golden_util import GOLDEN, case_digest
+    from uq_b200 import workloads as W
+
+    z = np.load(os.path.join(GOLDEN, "riemann256_500.npz"))
+    case = W.build("riemann", **json.loads(str(z["kwargs"])))
+    assert case_digest(case) == str(z["digest"])
+    o = O.Oracle(case)
+    o.step(int(z["step"]))
+    m = o.macro()
+    for k in ("rho", "T"):
+        assert rel_l2(m[k], z[k]) < 1e-8, (k, rel_l2(m[k], z[k]))
