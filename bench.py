@@ -485,6 +485,49 @@ def _alone_rate(rates, r, sides=(32, 128, 512, 1024)):
     return float(np.exp(np.interp(np.log(r["side"]), xs, ys)))
 
 
+def serving_saturated(n_requests=48, seed=777):
+    """The server's capacity: n_requests solves of the serving mix submitted
+    together at t = 0, makespan from the first submit to the last result in
+    host memory.  Against the same requests run one after another on the
+    plain FP64 path (rates per kind/method/side, interpolated)."""
+    from uq_b200.solver import Server
+
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for _ in range(n_requests):
+        kind = ["couette", "riemann"][int(rng.integers(0, 2))]
+        fm = int(rng.integers(0, 2))
+        reqs.append(dict(t=0.0, kind=kind, side=int(rng.integers(SERVE_SIDES[0], SERVE_SIDES[1] + 1)),
+                         steps=int(rng.integers(SERVE_STEPS[0], SERVE_STEPS[1] + 1)),
+                         fm=fm if kind == "couette" else 0, rk=int(rng.integers(0, 2)),
+                         seed=int(rng.integers(1 << 30))))
+    cases = [_serving_case(r) for r in reqs]
+    srv = Server(precision="f32")
+    warm = srv.submit(_serving_case(dict(kind="couette", side=64, steps=20, fm=1, rk=1, seed=3)))
+    srv.wait(warm)
+    srv.release(warm)
+    st0 = srv.stats()
+    t0 = time.perf_counter()
+    ids = [srv.submit(c) for c in cases]
+    codes = []
+    for rid in ids:
+        srv.wait(rid)
+        code, _ = srv.result(rid)
+        codes.append(int(code))
+        srv.release(rid)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lu = float(sum(r["side"] ** 2 * r["steps"] for r in reqs))
+    rates = _alone_fp64_rates()
+    alone = sum(r["side"] ** 2 * r["steps"] / (_alone_rate(rates, r) * 1e6) for r in reqs)
+    d = {k: st[k] - st0[k] for k in ("steps", "repacks", "graph_captures", "boundary_seconds", "capture_seconds",
+                                     "steps_eager", "steps_graph")}
+    return {"requests": n_requests, "completed_ok": int(sum(1 for c in codes if c == 0)), "makespan_s": wall,
+            "throughput_mlups": lu / wall / 1e6, "alone_fp64_sequential_mlups": lu / alone / 1e6,
+            "speedup_vs_alone_fp64_sequential": alone / wall, "server": d}
+
+
 def serving_probe(seconds, capacity_mlups, load=0.7, seed=4242):
     """Continuous-batching serving run: Poisson arrivals submitted in real
     time to one lbm_server (FP32), results collected as they finish.
@@ -558,7 +601,9 @@ def serving_probe(seconds, capacity_mlups, load=0.7, seed=4242):
         "aggregate_mlups": lu / (t_end - t0) / 1e6,
         "busy_mlups": st["lattice_updates"] / max(st["busy_seconds"], 1e-9) / 1e6,
         "alone_fp64_sequential_mlups": lu / float(alone.sum()) / 1e6,
-        "server": {k: st[k] for k in ("steps", "repacks", "compactions", "graph_captures", "arena_bytes")},
+        "server": {k: st[k] for k in ("steps", "repacks", "compactions", "graph_captures", "arena_bytes",
+                                      "boundary_seconds", "capture_seconds", "steps_eager", "steps_graph",
+                                      "busy_seconds")},
         "errors": errors,
     }
 
@@ -698,6 +743,10 @@ def run_ours(args, rank, world, local_rank):
             extra["serving"] = serving_probe(args.serving_seconds, value)
         except Exception as exc:  # reported, not fatal
             extra["serving"] = {"error": repr(exc)}
+        try:
+            extra["serving_saturated"] = serving_saturated()
+        except Exception as exc:  # reported, not fatal
+            extra["serving_saturated"] = {"error": repr(exc)}
 
     if rank == 0:
         out = {

@@ -301,6 +301,11 @@ typedef struct lbm_server_stats {
     size_t arena_bytes;
     double busy_seconds;        /* wall time with at least one resident solve */
     double uptime_seconds;
+    /* host time of the loop thread by part: step boundaries (retire, admit,
+     * repack, initialise), graph captures, and steps enqueued launch by
+     * launch (no graph yet) or replayed from a graph */
+    double boundary_seconds, capture_seconds;
+    long long steps_eager, steps_graph;
 } lbm_server_stats;
 
 LBM_API lbm_status lbm_server_create(const lbm_server_options *opt, lbm_server **out);

@@ -89,9 +89,10 @@ void prepare_sample(const HostSample &h, int prec, PreparedSample &out);
 // append the tx x ty tiles of one sample (flags in pitch layout) with the
 // given sample index; gid numbers continue from out.size()
 void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, int sample, std::vector<Tile> &out);
-// TMA descriptors of one sample's stage buffers 2 and 3
-void encode_stage_maps(int prec, const SampleParams &p, unsigned char *buf2, unsigned char *buf3, int tx, int ty,
-                       CUtensorMap *maps2);
+// TMA descriptors of one sample (MAPS_PER_SAMPLE of them): stage buffers 2
+// and 3 with the stencil halo box, and the state with the tile's own box
+void encode_stage_maps(int prec, const SampleParams &p, unsigned char *state, unsigned char *buf2,
+                       unsigned char *buf3, int tx, int ty, CUtensorMap *maps);
 void check_tile_shape(int x, int y);
 int round_up(int v, int m);
 

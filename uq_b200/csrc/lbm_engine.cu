@@ -340,22 +340,26 @@ void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, 
         }
 }
 
-// TMA descriptors: a sample's stage buffer 2 and 3, the 26 planes as a 3D
-// tensor (x, y, plane) with the staged halo box of the flux kernels.
-void encode_stage_maps(int prec, const SampleParams &p, unsigned char *buf2, unsigned char *buf3, int tx, int ty,
-                       CUtensorMap *maps2)
+// TMA descriptors of a sample, each over the 26 planes as a 3D tensor
+// (x, y, plane): stage buffers 2 and 3 with the flux kernels' staged halo
+// box (one plane), and the state with the tile's own nodes over
+// PREFETCH_PLANES planes (the update's reads of f or of h).
+void encode_stage_maps(int prec, const SampleParams &p, unsigned char *state, unsigned char *buf2,
+                       unsigned char *buf3, int tx, int ty, CUtensorMap *maps)
 {
     auto enc = tensor_map_encoder();
     const size_t es = prec == LBM_PREC_F64 ? 8 : 4;
-    for (int b = 0; b < 2; ++b) {
-        unsigned char *base = (b == 0 ? buf2 : buf3) + (size_t)p.state_off * es;
+    for (int b = 0; b < MAPS_PER_SAMPLE; ++b) {
+        unsigned char *base = (b == 0 ? buf2 : b == 1 ? buf3 : state) + (size_t)p.state_off * es;
         cuuint64_t dims[3] = {(cuuint64_t)p.nx, (cuuint64_t)p.ny, (cuuint64_t)NPL};
         cuuint64_t strides[2] = {(cuuint64_t)p.pitch * es, (cuuint64_t)p.plane * es};
-        cuuint32_t box[3] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 6), 1};
+        cuuint32_t halo[3] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 6), 1};
+        cuuint32_t own[3] = {(cuuint32_t)tx, (cuuint32_t)ty, (cuuint32_t)PREFETCH_PLANES};
         cuuint32_t estr[3] = {1, 1, 1};
-        CUresult r = enc(&maps2[b], prec == LBM_PREC_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-                         3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        CUresult r = enc(&maps[b], prec == LBM_PREC_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         3, base, dims, strides, b < 2 ? halo : own, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) throw LbmError(LBM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     }
 }
@@ -458,8 +462,9 @@ struct lbm_batch {
     void make_maps()
     {
         const int n = (int)hs.size();
-        std::vector<CUtensorMap> maps(2 * n);
-        for (int k = 0; k < n; ++k) encode_stage_maps(prec, sp[k], buf2.p, buf3.p, tx, ty, &maps[2 * k]);
+        std::vector<CUtensorMap> maps(MAPS_PER_SAMPLE * n);
+        for (int k = 0; k < n; ++k)
+            encode_stage_maps(prec, sp[k], state.p, buf2.p, buf3.p, tx, ty, &maps[MAPS_PER_SAMPLE * k]);
         d_maps.upload(maps, stream);
     }
 

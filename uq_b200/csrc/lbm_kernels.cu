@@ -76,22 +76,30 @@ __global__ void k_init(KArgs<S> a, const double *__restrict__ rho, const double 
 }
 
 // ------------------------------------------------------------------ moments
-// macroPropShort of one node: stn is the node's element in plane 0, the
-// planes sp.plane elements apart (offsets in a sample fit in 32 bits).
+// macroPropShort of one node from its 26 stored values, read through
+// rd(p) (p = i for f_i, NQ + i for h_i).
+template <class RD>
+__device__ __forceinline__ Macro node_macro_rd(RD rd, const SampleParams &sp)
+{
+    double r = 0, rux = 0, ruy = 0, sh = 0;
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+        const double fv = (double)rd(i);
+        r += fv;
+        rux += fv * (sp.c * c_EX[i]);
+        ruy += fv * (sp.c * c_EY[i]);
+        sh += (double)rd(NQ + i);
+    }
+    return macro_from_sums(r, rux, ruy, sh, sp);
+}
+
+// the same with stn the node's element in plane 0, the planes sp.plane
+// elements apart (offsets in a sample fit in 32 bits)
 template <class S>
 __device__ __forceinline__ Macro node_macro(const S *__restrict__ stn, const SampleParams &sp)
 {
     const int PL = (int)sp.plane;
-    double r = 0, rux = 0, ruy = 0, sh = 0;
-#pragma unroll
-    for (int i = 0; i < NQ; ++i) {
-        const double fv = (double)stn[i * PL];
-        r += fv;
-        rux += fv * (sp.c * c_EX[i]);
-        ruy += fv * (sp.c * c_EY[i]);
-        sh += (double)stn[(NQ + i) * PL];
-    }
-    return macro_from_sums(r, rux, ruy, sh, sp);
+    return node_macro_rd([&](int p) { return stn[p * PL]; }, sp);
 }
 
 // The same from the sample's plane 0 and the node's 64-bit offset o (the
@@ -250,9 +258,14 @@ struct FluxSmemLayout {
     size_t c_elems;      // C arrays: sf[2][G][4][NT], ring x[2][G][2][TY], ring y[2][G][2][TX], sD[26][NT]
     size_t stage_off;    // staged boxes
     size_t plane_bytes;  // one staged plane, padded to 128 bytes
-    size_t bar_off;      // NSTAGE mbarriers
+    size_t pref_off;     // the h half of the prefetched state (the f half lands in a freed staging slot)
+    size_t bar_off;      // NSTAGE mbarriers, then the prefetch's
     size_t total;        // including 128 bytes of base-alignment slack
 };
+
+// prefetch: the FP32 kernels load the update's state values of the tile
+// into shared memory while the last direction group is computed
+__host__ __device__ constexpr bool flux_prefetch(size_t es_s) { return es_s == 4; }
 
 __host__ __device__ inline FluxSmemLayout flux_layout(size_t es_c, size_t es_s, int tx, int ty, int G, int nstage)
 {
@@ -261,8 +274,10 @@ __host__ __device__ inline FluxSmemLayout flux_layout(size_t es_c, size_t es_s, 
     L.c_elems = 8 * (size_t)G * NT + 4 * (size_t)G * tx + 4 * (size_t)G * ty + (size_t)NPL * NT;
     L.stage_off = (L.c_elems * es_c + 127) / 128 * 128;
     L.plane_bytes = ((size_t)(tx + 2 * HALO_X) * (ty + 2 * HALO_Y) * es_s + 127) / 128 * 128;
-    L.bar_off = L.stage_off + (size_t)nstage * 2 * G * L.plane_bytes;
-    L.total = L.bar_off + nstage * sizeof(uint64_t) + 128;
+    L.pref_off = L.stage_off + (size_t)nstage * 2 * G * L.plane_bytes;
+    const size_t pref_bytes = flux_prefetch(es_s) ? ((size_t)PREFETCH_PLANES * NT * es_s + 127) / 128 * 128 : 0;
+    L.bar_off = L.pref_off + pref_bytes;
+    L.total = L.bar_off + (nstage + 1) * sizeof(uint64_t) + 128;
     return L;
 }
 
@@ -278,8 +293,10 @@ struct TileCtx {
     C *sD;           // [26][NT]
     const S *stg;    // [NSTAGE][G][2: f, h][BH][BW], planes `pstride` elements apart
     int pstride;
-    uint64_t *bars;  // [NSTAGE]
+    uint64_t *bars;  // [NSTAGE], then the prefetch's
     const CUtensorMap *map;
+    const CUtensorMap *smap;  // the state, box of the tile's own nodes over PREFETCH_PLANES planes
+    S *pref_h;                // where the h half of the prefetch lands
     int *timed_out;  // shared flag
     bool wrap_fix;   // general tiles: the box crosses a periodic edge
     int *status;     // this sample's status word
@@ -302,6 +319,21 @@ __device__ __forceinline__ void issue_group_load(TileCtx<S, C> &k, int g, int sl
         tma_load_3d(dst + (size_t)(2 * m) * k.pstride, k.map, k.x0 - HALO_X, k.y0 - HALO_Y, dir, &k.bars[slot]);
         tma_load_3d(dst + (size_t)(2 * m + 1) * k.pstride, k.map, k.x0 - HALO_X, k.y0 - HALO_Y, NQ + dir, &k.bars[slot]);
     }
+}
+
+// The update's state values of this tile (f planes into the freed staging
+// slot, h planes into their own region), completing on bars[NSTAGE]; the
+// slot's last readers passed the barrier before this is issued.
+template <int G, class S, class C>
+__device__ __forceinline__ void issue_state_prefetch(TileCtx<S, C> &k, int slot)
+{
+    const uint32_t bytes = (uint32_t)(k.NT * PREFETCH_PLANES * sizeof(S));
+    constexpr int NST = GroupCfg<G>::NSTAGE;
+    S *dst_f = const_cast<S *>(k.stg) + (size_t)slot * 2 * G * k.pstride;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&k.bars[NST], 2 * bytes);
+    tma_load_3d(dst_f, k.smap, k.x0, k.y0, 0, &k.bars[NST]);
+    tma_load_3d(k.pref_h, k.smap, k.x0, k.y0, NQ, &k.bars[NST]);
 }
 
 // reconstruction from the staged box (fast path; no solid, no domain edge
@@ -722,8 +754,11 @@ __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
         while (ring0 >= NT) ring0 -= NT;
     }
     __syncthreads();
-    // every thread is done with this slot: refill it NST groups ahead
+    // every thread is done with this slot: refill it NST groups ahead, or
+    // (the first slot that no later group needs) take the state prefetch
     if (g + NST < GroupCfg<G>::NGROUP && k.tid == 0) issue_group_load<G>(k, g + NST, slot);
+    else if (flux_prefetch(sizeof(S)) && g == GroupCfg<G>::NGROUP - NST && k.tid == 0)
+        issue_state_prefetch<G>(k, slot);
     if (SIMPLE || (k.active && (k.flag & NF_TYPE) == 0)) {
 #pragma unroll 1
         for (int m = 0; m < G; ++m) {
@@ -798,6 +833,8 @@ __device__ __forceinline__ void run_groups_c(TileCtx<S, C> &k)
         group_fluxes_c<S, C, FM, G, g, 0>(k, boxes, ring0);
         __syncthreads();
         if (g + NST < GroupCfg<G>::NGROUP && k.tid == 0) issue_group_load<G>(k, g + NST, slot);
+        else if (flux_prefetch(sizeof(S)) && g == GroupCfg<G>::NGROUP - NST && k.tid == 0)
+            issue_state_prefetch<G>(k, slot);
         group_divergence_c<S, C, G, g, 0>(k);
         run_groups_c<S, C, FM, G, g + 1>(k);
     }
@@ -847,16 +884,19 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     if (tile_simple(t) != (PATH == FLUX_SIMPLE)) return;
     const int tid = threadIdx.x;
     constexpr int PH = MODE == 2 ? 2 : 1;
-    const CUtensorMap *map = a.tmaps + 2 * t.sample + (PH == 1 ? 0 : 1);
+    const CUtensorMap *map = a.tmaps + MAPS_PER_SAMPLE * t.sample + (PH == 1 ? 0 : 1);
+    constexpr bool PREF = flux_prefetch(sizeof(S));
 
     TileCtx<S, C> k;
     k.NT = NT; k.TX = TX; k.TY = TY; k.BW = BW; k.BH = BH; k.tid = tid;
     k.x0 = t.x0; k.y0 = t.y0;
     k.stg = stg; k.pstride = (int)(Ls.plane_bytes / sizeof(S)); k.bars = bars; k.map = map; k.timed_out = &s_timeout;
+    k.smap = a.tmaps + MAPS_PER_SAMPLE * t.sample + 2;
+    k.pref_h = reinterpret_cast<S *>(smem_raw + Ls.pref_off);
     if (tid == 0) {
         s_sp = a.samples[t.sample];
         s_timeout = 0;
-        for (int b = 0; b < NST; ++b) mbar_init(&bars[b], 1);
+        for (int b = 0; b < NST + (PREF ? 1 : 0); ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
         for (int g = 0; g < NST; ++g) issue_group_load<G>(k, g, g);
     }
@@ -916,6 +956,16 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
         for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, false, G, -1>(k, g);
     }
 
+    // the prefetched state values: every thread waits (boundedly) for the
+    // copies, so that none is in flight when the block exits
+    const S *pref_f = nullptr;
+    if constexpr (PREF) {
+        if (!mbar_wait_bounded(&bars[NST], 0, TMA_WAIT_POLLS)) {
+            s_timeout = 1;
+            atomicOr(&a.status[t.sample], STATUS_TIMEOUT);
+        }
+        pref_f = stg + (size_t)((GroupCfg<G>::NGROUP - NST) % NST) * 2 * G * k.pstride;
+    }
     double res_part = 0;
     if (active && type == 0) {
         // this node in plane 0 of each buffer; planes PL elements apart
@@ -923,6 +973,13 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
         const S *__restrict__ b2 = a.buf2 + sp.state_off + o;
         S *__restrict__ b3 = a.buf3 + sp.state_off + o;
         const int PL = (int)sp.plane;
+        // the node's state value of plane p at the start of the update: from
+        // the prefetch (FP32) or from memory
+        const S *pref_h = k.pref_h;
+        auto rd = [&](int p) -> S {
+            if constexpr (PREF) return p < NQ ? pref_f[p * NT + tid] : pref_h[(p - NQ) * NT + tid];
+            else return st[p * PL];
+        };
         const C dt = (C)sp.dt;
         bool final_phase = true;
         double fin_r = 0, fin_sh = 0;  // FP64 sums of the new state (MODE 2)
@@ -937,19 +994,19 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             C rq1, rq3, ux1, uy1, ux3, uy3;
             double rho3;
             {
-                m1 = node_macro(st, sp);
+                m1 = node_macro_rd(rd, sp);
                 rq1 = (C)m1.q; ux1 = (C)m1.ux; uy1 = (C)m1.uy;
             }
             {
                 double r = 0, rux = 0, ruy = 0, sh = 0;
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) {
-                    const double fv = (double)st[i * PL];
+                    const double fv = (double)rd(i);
                     const double Df = (double)sD[i * NT + tid];
                     r += fv - Df;
                     rux += fv * (sp.c * c_EX[i]) - Df * (sp.c * c_EX[i]);
                     ruy += fv * (sp.c * c_EY[i]) - Df * (sp.c * c_EY[i]);
-                    sh += (double)st[(NQ + i) * PL] - (double)sD[(NQ + i) * NT + tid];
+                    sh += (double)rd(NQ + i) - (double)sD[(NQ + i) * NT + tid];
                 }
                 m3 = macro_from_sums(r, rux, ruy, sh, sp);
                 rq3 = (C)m3.q; ux3 = (C)m3.ux; uy3 = (C)m3.uy;
@@ -975,7 +1032,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                 for (int k = 0; k < 4; ++k) {
                     if (k >= n) break;
                     const int of = (i0 + k) * PL, oh = (NQ + i0 + k) * PL;
-                    vf[k] = (C)st[of]; vh[k] = (C)st[oh]; vf2[k] = (C)b2[of]; vh2[k] = (C)b2[oh];
+                    vf[k] = (C)rd(i0 + k); vh[k] = (C)rd(NQ + i0 + k); vf2[k] = (C)b2[of]; vh2[k] = (C)b2[oh];
                 }
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
@@ -1017,7 +1074,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             for (int half = 0; half < 2; ++half) {
                 S acc[NQ];
 #pragma unroll
-                for (int i = 0; i < NQ; ++i) acc[i] = st[(half * NQ + i) * PL];
+                for (int i = 0; i < NQ; ++i) acc[i] = rd(half * NQ + i);
                 // NaN / Inf propagate through an FP32 sum as through an FP64 one
                 typename std::conditional<sizeof(S) == 4, float, double>::type sum = 0;
 #pragma unroll
@@ -1031,7 +1088,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             }
         } else {
             // RK1 update (cpuLBM.cpp:1674-1710), EULER (:2130-2168), EULER_EQ (:2220-2258)
-            const Macro m = node_macro(st, sp);
+            const Macro m = node_macro_rd(rd, sp);
             constexpr bool DEV = sizeof(S) == 4;
             const EqArgs<C, DEV> q(m.rho, m.ux, m.uy, m.T, sp);
             const C ux = (C)m.ux, uy = (C)m.uy, Pr = (C)sp.Pr;
@@ -1046,7 +1103,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                 for (int k = 0; k < 4; ++k) {
                     if (k >= n) break;
                     const int of = (i0 + k) * PL, oh = (NQ + i0 + k) * PL;
-                    vf[k] = (C)st[of]; vh[k] = (C)st[oh];
+                    vf[k] = (C)rd(i0 + k); vh[k] = (C)rd(NQ + i0 + k);
                     if (MODE == 3) { v1f[k] = (C)b2[of]; v1h[k] = (C)b2[oh]; }
                 }
 #pragma unroll

@@ -16,6 +16,12 @@ constexpr int STATUS_EQ = 1;         // equilibrium mass check (cpuLBM.cpp:839-8
 constexpr int STATUS_NONFINITE = 2;  // NaN / Inf / rho <= 0 in the state
 constexpr int STATUS_TIMEOUT = 4;    // a bounded device-side wait ran out
 
+// tensor maps per sample: the stage buffers 2 and 3 with the stencil
+// kernels' halo box, and the state with a box of the tile's own nodes over
+// 13 planes (the f or the h half of the state, prefetched for the update)
+constexpr int MAPS_PER_SAMPLE = 3;
+constexpr int PREFETCH_PLANES = 13;
+
 struct WallNode {
     int sample, x, y, pad;
 };
@@ -36,7 +42,7 @@ struct KArgs {
     double *partial;  // per-tile residual partial sums
     int *status;      // per-sample status bits
     const double *tdx, *tdy, *dxv, *dyv;
-    const CUtensorMap *tmaps;  // per sample: [buffer 2, buffer 3]
+    const CUtensorMap *tmaps;  // per sample MAPS_PER_SAMPLE maps: [buffer 2, buffer 3, state]
     const double *fref;        // per sample: 26 rest-state values subtracted from the stored state
     int want_residual;
     double eq_tol;

@@ -365,7 +365,7 @@ struct lbm_server {
         v_dx.clear();
         v_dy.clear();
         v_fref.clear();
-        maps.resize(2 * packed.size());
+        maps.resize(MAPS_PER_SAMPLE * packed.size());
         packed_nodes = 0;
         for (size_t k = 0; k < packed.size(); ++k) {
             Request *r = packed[k];
@@ -396,7 +396,7 @@ struct lbm_server {
             v_dx.insert(v_dx.end(), r->ps.dx.begin(), r->ps.dx.end());
             v_dy.insert(v_dy.end(), r->ps.dy.begin(), r->ps.dy.end());
             v_fref.insert(v_fref.end(), r->ps.fref, r->ps.fref + NPL);
-            encode_stage_maps(prec, p, buf2.p, buf3.p, tx, ty, &maps[2 * k]);
+            encode_stage_maps(prec, p, state.p, buf2.p, buf3.p, tx, ty, &maps[MAPS_PER_SAMPLE * k]);
             sp.push_back(p);
             packed_nodes += (long long)r->nx * r->ny;
         }
@@ -509,6 +509,7 @@ struct lbm_server {
         const int slot = (int)(steps_enqueued % kRunAhead);
         if (steps_enqueued >= kRunAhead) CU(cudaEventSynchronize(ev_step[slot]));
         if (use_graph && !graph && stable_steps >= 2) {
+            const auto t0 = Clock::now();
             cudaGraph_t g;
             CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
             try {
@@ -521,9 +522,15 @@ struct lbm_server {
             CU(cudaGraphInstantiate(&graph, g, 0));
             cudaGraphDestroy(g);
             stats.graph_captures++;
+            stats.capture_seconds += std::chrono::duration<double>(Clock::now() - t0).count();
         }
-        if (graph) CU(cudaGraphLaunch(graph, stream));
-        else enqueue_one_step();
+        if (graph) {
+            CU(cudaGraphLaunch(graph, stream));
+            stats.steps_graph++;
+        } else {
+            enqueue_one_step();
+            stats.steps_eager++;
+        }
         CU(cudaEventRecord(ev_step[slot], stream));
         steps_enqueued++;
         stable_steps++;
@@ -690,7 +697,11 @@ struct lbm_server {
                     continue;
                 }
             }
-            if (!leaving.empty() || !joining.empty() || rebuild_needed) boundary(leaving, staying, joining);
+            if (!leaving.empty() || !joining.empty() || rebuild_needed) {
+                const auto t0 = Clock::now();
+                boundary(leaving, staying, joining);
+                stats.boundary_seconds += std::chrono::duration<double>(Clock::now() - t0).count();
+            }
             rebuild_needed = false;
             if (packed.empty()) continue;
             step_once();

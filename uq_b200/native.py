@@ -84,7 +84,9 @@ class LbmServerStats(C.Structure):
                 ("lattice_updates", C.c_longlong), ("repacks", C.c_longlong), ("compactions", C.c_longlong),
                 ("graph_captures", C.c_longlong), ("resident", C.c_int), ("queued", C.c_int),
                 ("arena_nodes", C.c_longlong), ("arena_nodes_used", C.c_longlong), ("arena_bytes", C.c_size_t),
-                ("busy_seconds", C.c_double), ("uptime_seconds", C.c_double)]
+                ("busy_seconds", C.c_double), ("uptime_seconds", C.c_double),
+                ("boundary_seconds", C.c_double), ("capture_seconds", C.c_double),
+                ("steps_eager", C.c_longlong), ("steps_graph", C.c_longlong)]
 
 
 # name -> (restype, argtypes); every function include/uq_lbm.h declares
