@@ -836,6 +836,21 @@ void orc_set_dist(orc *s, const double *f, const double *h)
         for (int y = 0; y < s->Ny; ++y) macro_short(s, x, y);
 }
 
+/* the viscosity law alone at temperature T, with the parameters set as
+ * orc_create sets them (for pinning against the reference's OpenCL
+ * generator, codeCL.py:60-69, 986-990) */
+double orc_viscosity(int mu_model, double mu_ref, double T_ref, double upsilon, double S_v, double T)
+{
+    orc s;
+    memset(&s, 0, sizeof s);
+    s.mu_model = mu_model;
+    s.mu = mu_ref;
+    s.T_ref = T_ref;
+    s.S_v = S_v;
+    s.visc_exp = mu_model == 1 ? 0.5 + upsilon : 1.5;
+    return viscosity(&s, T);
+}
+
 double orc_dt(const orc *s) { return s->dt; }
 int orc_nsteps(const orc *s) { return s->nsteps; }
 int orc_step_count(const orc *s) { return s->step; }

@@ -57,6 +57,7 @@ int orc_run(orc *s, int max_steps, double *residual_trace);
 void orc_get_macro(const orc *s, double *rho, double *ux, double *uy, double *T, double *p);
 void orc_get_dist(const orc *s, double *f, double *h);
 void orc_set_dist(orc *s, const double *f, const double *h);
+double orc_viscosity(int mu_model, double mu_ref, double T_ref, double upsilon, double S_v, double T);
 double orc_dt(const orc *s);
 int orc_nsteps(const orc *s);
 int orc_step_count(const orc *s);

@@ -62,8 +62,18 @@ def lib():
         L.orc_residual.restype = C.c_double
         L.orc_residual.argtypes = [C.c_void_p]
         L.orc_equilibrium.argtypes = [C.c_double] * 7 + [_dp, _dp]
+        L.orc_viscosity.restype = C.c_double
+        L.orc_viscosity.argtypes = [C.c_int] + [C.c_double] * 5
         _lib = L
     return _lib
+
+
+def viscosity(mu_model, mu_ref, T_ref, upsilon, S_v, T):
+    """The oracle's viscosity law (0 constant, 1 VHS, 2 Sutherland) at each
+    temperature of T."""
+    L = lib()
+    return np.array([L.orc_viscosity(int(mu_model), float(mu_ref), float(T_ref), float(upsilon), float(S_v),
+                                     float(t)) for t in np.ravel(T)])
 
 
 def _d(a):

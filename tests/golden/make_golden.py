@@ -12,6 +12,8 @@ checksum of that input to catch builder drift.
     python tests/golden/make_golden.py chaos    # only the 1-ulp perturbation fixture
     python tests/golden/make_golden.py riemann  # only the Riemann 256^2 fixture
     python tests/golden/make_golden.py ensemble # only the ensemble's 64^2 status fixture
+    python tests/golden/make_golden.py spread   # only the single-precision spread fixture
+    python tests/golden/make_golden.py viscosity  # the viscosity laws from the reference's OpenCL generator
 
 Needs the reference tree (only in the development container); the fixtures
 themselves are committed and need nothing at test time.
@@ -191,9 +193,23 @@ def riemann_floor():
 
 def _ref_status(args):
     """Reference run of one ensemble sample to `steps` steps: (stop flag,
-    steps done, all fields finite)."""
-    sample, steps = args
-    r = refrun.run_reference(W.ensemble_case(sample), max_steps=steps)
+    steps done, all fields finite); perturbed: every interior density moved
+    by 1 ulp (seeded signs) first.  A run that the reference binary does not
+    survive (it dies of a signal on some diverging states) is recorded as
+    stop -1, step -1."""
+    sample, steps, perturbed = args
+    case = W.ensemble_case(sample)
+    if perturbed:
+        rng = np.random.default_rng(77)
+        d = case["density"].copy()
+        d[2:] = np.nextafter(d[2:], rng.choice([-np.inf, np.inf], size=d.size - 2))
+        case["density"] = d
+    import subprocess
+
+    try:
+        r = refrun.run_reference(case, max_steps=steps)
+    except subprocess.CalledProcessError:
+        return -1, -1, False
     finite = all(np.all(np.isfinite(r[k])) for k in ("rho", "ux", "uy", "T"))
     return int(r["stop"]), int(r["step"]), bool(finite)
 
@@ -203,26 +219,157 @@ def ensemble_status(side=64, steps=1000, seed=1234, n=512):
     u_w ~ U(0.05, 0.2), tau ~ U(0.02, 0.1), Pr ~ U(0.6, 1.0), WENO5, RK3):
     what the reference's driver reports after `steps` steps for each --
     stop (1: runOne's hasFailed, the equilibrium check) and the step it
-    stopped at."""
+    stopped at -- and the same for a second reference run whose interior
+    densities differ by 1 ulp (how much of that record rounding decides)."""
     import concurrent.futures as cf
     import multiprocessing as mp
 
     samples = W.uq_ensemble(n=n, seed=seed)
     picks = [(k, d) for k, d in enumerate(samples) if d["nx"] == side]
     with cf.ProcessPoolExecutor(max_workers=os.cpu_count() or 1, mp_context=mp.get_context("spawn")) as ex:
-        res = list(ex.map(_ref_status, [(d, steps) for _, d in picks]))
+        res = list(ex.map(_ref_status, [(d, steps, False) for _, d in picks]))
+        res_p = list(ex.map(_ref_status, [(d, steps, True) for _, d in picks]))
     arrays = {"index": np.array([k for k, _ in picks]), "side": np.array(side), "steps": np.array(steps),
               "seed": np.array(seed), "n": np.array(n),
               "u_w": np.array([d["u_w"] for _, d in picks]), "tau": np.array([d["tau"] for _, d in picks]),
               "Pr": np.array([d["Pr"] for _, d in picks]),
               "stop": np.array([r[0] for r in res]), "step": np.array([r[1] for r in res]),
-              "finite": np.array([r[2] for r in res])}
+              "finite": np.array([r[2] for r in res]),
+              "stop_ulp": np.array([r[0] for r in res_p]), "step_ulp": np.array([r[1] for r in res_p])}
     np.savez_compressed(os.path.join(OUT, "ensemble%d_status.npz" % side), **arrays)
-    print("ensemble%d_status.npz: %d samples, %d stopped by the equilibrium check" %
-          (side, len(picks), int((arrays["stop"] == 1).sum())))
+    fail, fail_p = arrays["stop"] != 2, arrays["stop_ulp"] != 2
+    print("ensemble%d_status.npz: %d samples, %d did not complete (%d crashed); 1-ulp run %d (%d crashed), "
+          "disagreeing on %d" % (side, len(picks), int(fail.sum()), int((arrays["stop"] == -1).sum()),
+                                 int(fail_p.sum()), int((arrays["stop_ulp"] == -1).sum()), int((fail != fail_p).sum())))
+
+
+def per_node_ids(case):
+    """The same case with every node its own property id (same values), so
+    that each node's inputs can be changed alone."""
+    bnd = np.asarray(case["bnd"])
+    out = dict(case)
+    for k in ("density", "pressure", "temp", "velocityX", "velocityY", "cellType"):
+        out[k] = np.asarray(case[k])[bnd.reshape(-1)]
+    out["numProps"] = bnd.size
+    out["bnd"] = np.arange(bnd.size, dtype=np.int64).reshape(bnd.shape)
+    return out
+
+
+def f32ulp_perturbed(case, seed=77):
+    """Every non-solid node's density moved by one single-precision ulp
+    (relative 2^-24), up or down with seeded signs."""
+    c = per_node_ids(case)
+    rng = np.random.default_rng(seed)
+    d = np.asarray(c["density"], dtype=np.float64).copy()
+    move = np.asarray(c["cellType"]) != 2
+    d[move] *= 1.0 + rng.choice([-1.0, 1.0], size=int(move.sum())) * 2.0 ** -24
+    c["density"] = d
+    return c
+
+
+def _ref_macro(args):
+    case, steps = args
+    r = refrun.run_reference(case, max_steps=steps)
+    return {k: r[k] for k in ("rho", "ux", "uy", "T")}
+
+
+def f32_spread():
+    """How far the reference moves, on each short-horizon fixture case, when
+    every node's density changes by one single-precision ulp: the relative
+    L2 of rho, u, T of that run against the unperturbed one (the committed
+    fixture's fields, which the per-node-id case reproduces bit for bit).
+    Cases: couette16.npz (6 schemes, 50 steps), riemann32.npz (2 cases),
+    riemann256_500.npz."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    jobs, refs, names = [], [], []
+    for fname in ("couette16.npz", "riemann32.npz"):
+        z = np.load(os.path.join(OUT, fname))
+        metas = json.loads(str(z["meta"]))
+        for k, meta in enumerate(metas):
+            case = W.build(meta["builder"], **meta["kwargs"])
+            steps = int(z["c%d_step" % k])
+            jobs += [(per_node_ids(case), steps), (f32ulp_perturbed(case), steps)]
+            refs.append({f: z["c%d_%s" % (k, f)] for f in ("rho", "ux", "uy", "T")})
+            names.append("%s[%d]" % (fname, k))
+    z = np.load(os.path.join(OUT, "riemann256_500.npz"))
+    case = W.build("riemann", **json.loads(str(z["kwargs"])))
+    jobs += [(per_node_ids(case), int(z["step"])), (f32ulp_perturbed(case), int(z["step"]))]
+    refs.append({f: z[f] for f in ("rho", "ux", "uy", "T")})
+    names.append("riemann256_500.npz")
+    with cf.ProcessPoolExecutor(max_workers=os.cpu_count() or 1, mp_context=mp.get_context("spawn")) as ex:
+        res = list(ex.map(_ref_macro, jobs))
+    errs = []
+    for j, name in enumerate(names):
+        same, pert = res[2 * j], res[2 * j + 1]
+        for f in ("rho", "ux", "uy", "T"):
+            assert np.array_equal(same[f], refs[j][f]), (name, f)  # per-node ids change nothing
+        errs.append(_l2_errors(pert, refs[j]))
+        print(name, "FP32-ulp spread (rho, u, T):", ["%.2e" % e for e in errs[-1]])
+    np.savez_compressed(os.path.join(OUT, "f32_spread.npz"), names=np.array(names), err=np.array(errs),
+                        perturb_seed=np.array(77))
+
+
+VISCOSITY_LAWS = (dict(model="VHS", mu_ref=0.05, T_ref=1.0, upsilon=0.25),
+                  dict(model="VHS", mu_ref=1.8e-5, T_ref=273.0, upsilon=0.31),
+                  dict(model="sutherland", mu_ref=0.05, T_ref=1.0, S_v=0.4),
+                  dict(model="sutherland", mu_ref=1.716e-5, T_ref=273.15, S_v=110.4))
+
+
+def viscosity_laws():
+    """The viscosity laws as the reference's own OpenCL generator writes them
+    (CODE/Python/simLB/codeCL.py: genOpenCL, 60-69 and 986-990): the
+    generator runs in a temporary directory (it writes kernel.cl there) for
+    each law, every `double mu = ...;` line it emits is collected (all must
+    be the same expression), and the expression is evaluated with the
+    constants it emits over a grid of temperatures.  The fixture keeps the
+    expressions and the values."""
+    import importlib.util
+    import math
+    import re
+    import tempfile
+
+    spec = importlib.util.spec_from_file_location(
+        "ref_codeCL", os.path.join(REF_ROOT, "CODE", "Python", "simLB", "codeCL.py"))
+    codeCL = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(codeCL)
+    ex = [0, 1, 0, -1, 0, 1, -1, -1, 1, 2, 0, -2, 0]
+    ey = [0, 0, 1, 0, -1, 1, 1, -1, -1, 0, 2, 0, -2]
+    inp = dict(Nx=8, Ny=8, Ni=13, FMETHOD=1, RKMETHOD=1, K=3.0, Pr=0.71, R=1.0, Tc=1.0, b=5.0, dt=0.25,
+               isSolid=0, mirrorE=0, mirrorN=0, mirrorS=0, mirrorW=0, periodicX=1, periodicY=0)
+    cwd = os.getcwd()
+    arrays, exprs = {}, []
+    for j, law in enumerate(VISCOSITY_LAWS):
+        with tempfile.TemporaryDirectory(prefix="gencl_") as tmp:
+            os.chdir(tmp)
+            try:
+                codeCL.genOpenCL(dict(inp), dict(law), ex, ey, [1.0] * inp["Nx"], [1.0] * inp["Ny"])
+                src = open("kernel.cl").read()
+            finally:
+                os.chdir(cwd)
+        consts = {m.group(1): float(m.group(2))
+                  for m in re.finditer(r"__constant double (\w+) = ([-+0-9.eE]+);", src)}
+        lines = sorted({m.group(1).strip() for m in re.finditer(r"double mu = (.+);", src)})
+        # the laws use T (or T2, the same temperature, in one kernel)
+        forms = sorted({ln.replace("T2", "T") for ln in lines})
+        assert len(forms) == 1, forms
+        T = np.linspace(0.2, 3.0, 57) * law["T_ref"]
+        env = dict(consts, powr=math.pow)
+        mu = np.array([eval(forms[0], {"__builtins__": {}}, dict(env, T=t)) for t in T])
+        exprs.append(dict(law, expression=forms[0], constants=consts))
+        arrays["T%d" % j] = T
+        arrays["mu%d" % j] = mu
+    arrays["laws"] = np.array(json.dumps(exprs))
+    np.savez_compressed(os.path.join(OUT, "viscosity_laws.npz"), **arrays)
+    for e in exprs:
+        print("viscosity_laws.npz:", e["model"], e["expression"])
 
 
 def main():
+    if sys.argv[1:] == ["viscosity"]:  # needs only the reference's Python sources
+        viscosity_laws()
+        return
     if not refrun.available():
         sys.exit("reference binary missing: make -C oracle")
     if sys.argv[1:] == ["mat"]:
@@ -236,6 +383,9 @@ def main():
         return
     if sys.argv[1:] == ["ensemble"]:
         ensemble_status()
+        return
+    if sys.argv[1:] == ["spread"]:
+        f32_spread()
         return
 
     # (i) two steps from seeded random states: every BC family x flux x stepper
@@ -285,6 +435,8 @@ def main():
     chaos()
     riemann_floor()
     ensemble_status()
+    f32_spread()
+    viscosity_laws()
 
 
 if __name__ == "__main__":

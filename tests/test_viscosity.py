@@ -35,3 +35,24 @@ def test_laws_change_a_flow_with_varying_temperature():
         f1, _ = _run(_case(**law))
         d = np.max(np.abs(f1 - f0)) / np.max(np.abs(f0))
         assert 1e-8 < d < 1e-1, (law, d)
+
+
+def test_laws_match_the_reference_generator():
+    """The oracle's laws against the expressions the reference's own OpenCL
+    generator emits (tests/golden/viscosity_laws.npz, made by running
+    genOpenCL of CODE/Python/simLB/codeCL.py for a VHS and a Sutherland
+    configuration and evaluating the `double mu = ...;` lines it writes).
+    The GPU paths match the oracle for both laws (test_gpu_viscosity.py)."""
+    import json
+    import os
+
+    from golden_util import GOLDEN
+
+    z = np.load(os.path.join(GOLDEN, "viscosity_laws.npz"))
+    laws = json.loads(str(z["laws"]))
+    assert {law["model"] for law in laws} == {"VHS", "sutherland"}
+    for j, law in enumerate(laws):
+        model = 1 if law["model"] == "VHS" else 2
+        c = law["constants"]
+        mu = O.viscosity(model, c["mu_ref"], c["T_ref"], c.get("upsilon", 0.0), c.get("S_v", 0.0), z["T%d" % j])
+        np.testing.assert_allclose(mu, z["mu%d" % j], rtol=1e-15, atol=0, err_msg=law["expression"])
