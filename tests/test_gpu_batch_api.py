@@ -26,10 +26,12 @@ def test_profile_and_launch_count(cuda_device):
     b = Batch([W.couette(nx=64, ny=48, steps=4, seed=1)], "f32")
     ms = b.profile(2)
     assert ms.shape == (6,) and (ms[:5] >= 0).all() and ms[2] > 0
-    # 4 x 3 tiles of 16 x 16, two of them simple: pointwise, walls, stencil
-    # 1 (simple and general kernels), walls, stencil 2 (both), + residual
-    assert b.launches_per_step(False) == 7
-    assert b.launches_per_step(True) == 8
+    # 4 x 3 tiles of 16 x 16: in the middle row two simple tiles and, at the
+    # periodic edges, two wrap tiles; the rest touch the walls.  Pointwise,
+    # walls, stencil 1 (simple, wrap and general kernels), walls, stencil 2
+    # (all three), + residual
+    assert b.launches_per_step(False) == 9
+    assert b.launches_per_step(True) == 10
 
 
 def test_tile_shape_does_not_change_results(cuda_device):
@@ -58,3 +60,29 @@ def test_autotune_keeps_state_and_results(cuda_device):
     b.step(3)
     for k in range(2):
         assert np.array_equal(a.dist(k)[0], b.dist(k)[0])
+
+
+def test_wrap_tiles_match_oracle(cuda_device):
+    """Tiles at periodic edges whose halo holds only plain fluid run the
+    simple-tile code on a staged box completed with the periodic images:
+    periodic in x (Couette) and in both axes (a smooth random state), FP64
+    against the oracle and FP32 within the mixed-path tolerance."""
+    from oracle import oracle as O
+
+    cases = [W.couette(nx=64, ny=48, steps=6, seed=5),
+             W.random_state(64, 48, seed=6, bc="periodic", du=0.01, drho=0.01, dT=0.01, steps=6)]
+    b = Batch(cases, "f64")
+    assert b.launches_per_step(False) == 9  # a wrap run in each stencil phase
+    b.step(6)
+    b32 = Batch(cases, "f32")
+    b32.step(6)
+    for k, c in enumerate(cases):
+        o = O.Oracle(c)
+        o.step(6)
+        f, h = b.dist(k)
+        fo, ho = o.dist()
+        assert np.linalg.norm(f - fo) / np.linalg.norm(fo) < 1e-11, k
+        assert np.linalg.norm(h - ho) / np.linalg.norm(ho) < 1e-11, k
+        m, mo = b32.macro(k), o.macro()
+        for q in ("rho", "T"):
+            assert np.linalg.norm(m[q] - mo[q]) / np.linalg.norm(mo[q]) < 1e-5, (k, q)

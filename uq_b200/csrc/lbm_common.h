@@ -86,9 +86,11 @@ struct PreparedSample {
 
 HostSample derive(const lbm_config &c, const lbm_init &in);
 void prepare_sample(const HostSample &h, int prec, PreparedSample &out);
-// append the tx x ty tiles of one sample (flags in pitch layout) with the
-// given sample index; gid numbers continue from out.size()
-void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, int sample, std::vector<Tile> &out);
+// append the tx x ty tiles of one sample (flags in pitch layout, sample
+// flags sflags for its periodic axes) with the given sample index; gid
+// numbers continue from out.size()
+void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, int sflags, int sample,
+               std::vector<Tile> &out);
 // TMA descriptors of one sample (MAPS_PER_SAMPLE of them): stage buffers 2
 // and 3 with the stencil halo box, and the state with the tile's own box
 void encode_stage_maps(int prec, const SampleParams &p, unsigned char *state, unsigned char *buf2,
@@ -104,36 +106,46 @@ struct TileRun {
 
 // Device pointers and lengths of the packed lists one step launches over.
 // The pointwise phase runs over the tiles of each RKMETHOD in sample order;
-// the stencil phases over the same tiles as two runs, the simple tiles and
-// the rest, one kernel per run, each compiled for its kind of tile alone.
+// the stencil phases over the same tiles as three runs, the simple tiles,
+// the wrap tiles and the rest, one kernel per run, each compiled for its
+// kind of tile alone.
 struct StepLists {
-    TileRun pointwise[4];              // tiles by RKMETHOD, sample order
-    TileRun simple[4], general[4];     // the same tiles by kind
-    TileRun rk3_simple, rk3_general;   // RK3 tiles (final stencil phase)
+    TileRun pointwise[4];                           // tiles by RKMETHOD, sample order
+    TileRun simple[4], wrap[4], general[4];         // the same tiles by kind
+    TileRun rk3_simple, rk3_wrap, rk3_general;      // RK3 tiles (final stencil phase)
     const WallNode *walls_all = nullptr, *walls_rk3 = nullptr;
     int n_walls_all = 0, n_walls_rk3 = 0;
 };
 
-// A device list of n tiles whose first ns are simple, as two runs.
-inline void split_runs(const Tile *p, int n, int ns, TileRun &simple, TileRun &general)
+// A device list of n tiles whose first ns are simple and next nw wrap
+// tiles, as three runs.
+inline void split_runs(const Tile *p, int n, int ns, int nw, TileRun &simple, TileRun &wrap, TileRun &general)
 {
     simple.p = p;
     simple.n = ns;
-    general.p = p ? p + ns : nullptr;
-    general.n = n - ns;
+    wrap.p = p ? p + ns : nullptr;
+    wrap.n = nw;
+    general.p = p ? p + ns + nw : nullptr;
+    general.n = n - ns - nw;
 }
 
-// Reorder a host tile list so that its simple tiles come first (each kind
-// keeps its order); returns how many are simple.
-inline int simple_first(std::vector<Tile> &v)
+// Reorder a host tile list by kind, simple tiles first, then wrap tiles,
+// then the rest (each kind keeps its order); ns, nw: how many are simple
+// and wrap tiles.
+inline void order_by_kind(std::vector<Tile> &v, int &ns, int &nw)
 {
-    return (int)(std::stable_partition(v.begin(), v.end(), [](const Tile &t) { return tile_simple(t); }) - v.begin());
+    auto mid = std::stable_partition(v.begin(), v.end(), [](const Tile &t) { return tile_simple(t); });
+    auto end = std::stable_partition(mid, v.end(), [](const Tile &t) { return tile_wrap(t); });
+    ns = (int)(mid - v.begin());
+    nw = (int)(end - mid);
 }
 
 template <class S, class C>
-void stencil_runs(const KArgs<S> &a, int phase, int m, const TileRun &s, const TileRun &g, cudaStream_t st)
+void stencil_runs(const KArgs<S> &a, int phase, int m, const TileRun &s, const TileRun &w, const TileRun &g,
+                  cudaStream_t st)
 {
     if (s.n) CU((launch_phase<S, C>(a, phase, m, s.p, s.n, nullptr, 0, st, FLUX_SIMPLE)));
+    if (w.n) CU((launch_phase<S, C>(a, phase, m, w.p, w.n, nullptr, 0, st, FLUX_WRAP)));
     if (g.n) CU((launch_phase<S, C>(a, phase, m, g.p, g.n, nullptr, 0, st, FLUX_GENERAL)));
 }
 
@@ -149,12 +161,12 @@ void enqueue_step_phases(const KArgs<S> &a, const StepLists &l, cudaStream_t st,
     if (ev) CU(cudaEventRecord(ev[1], st));
     CU((launch_phase<S, C>(a, 3, 0, nullptr, 0, l.walls_all, l.n_walls_all, st)));
     if (ev) CU(cudaEventRecord(ev[2], st));
-    for (int m = 0; m < 4; ++m) stencil_runs<S, C>(a, 1, m, l.simple[m], l.general[m], st);
+    for (int m = 0; m < 4; ++m) stencil_runs<S, C>(a, 1, m, l.simple[m], l.wrap[m], l.general[m], st);
     if (ev) CU(cudaEventRecord(ev[3], st));
-    const bool rk3 = l.rk3_simple.n || l.rk3_general.n;
+    const bool rk3 = l.rk3_simple.n || l.rk3_wrap.n || l.rk3_general.n;
     if (rk3) CU((launch_phase<S, C>(a, 4, 1, nullptr, 0, l.walls_rk3, l.n_walls_rk3, st)));
     if (ev) CU(cudaEventRecord(ev[4], st));
-    if (rk3) stencil_runs<S, C>(a, 2, 1, l.rk3_simple, l.rk3_general, st);
+    if (rk3) stencil_runs<S, C>(a, 2, 1, l.rk3_simple, l.rk3_wrap, l.rk3_general, st);
     if (ev) CU(cudaEventRecord(ev[5], st));
 }
 
@@ -162,10 +174,10 @@ inline int step_launches(const StepLists &l)
 {
     int n = 0;
     for (int m = 0; m < 4; ++m)
-        n += (l.pointwise[m].n ? 1 : 0) + (l.simple[m].n ? 1 : 0) + (l.general[m].n ? 1 : 0);
+        n += (l.pointwise[m].n ? 1 : 0) + (l.simple[m].n ? 1 : 0) + (l.wrap[m].n ? 1 : 0) + (l.general[m].n ? 1 : 0);
     n += l.n_walls_all ? 1 : 0;
-    if (l.rk3_simple.n || l.rk3_general.n)
-        n += (l.n_walls_rk3 ? 1 : 0) + (l.rk3_simple.n ? 1 : 0) + (l.rk3_general.n ? 1 : 0);
+    if (l.rk3_simple.n || l.rk3_wrap.n || l.rk3_general.n)
+        n += (l.n_walls_rk3 ? 1 : 0) + (l.rk3_simple.n ? 1 : 0) + (l.rk3_wrap.n ? 1 : 0) + (l.rk3_general.n ? 1 : 0);
     return n;
 }
 

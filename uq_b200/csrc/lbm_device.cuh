@@ -60,9 +60,15 @@ struct Tile {
 // A simple tile lies at least 3 nodes inside its domain and neither it nor
 // its 3-node halo holds a solid/permanent node or a node whose stencil meets
 // a solid or an edge: every flux it needs comes straight from the staged box.
+// A wrap tile is a full tile that would be simple but for a periodic edge:
+// its halo crosses it (along a periodic axis) and holds only plain fluid
+// nodes, so once the periodic images are copied into the staged box every
+// flux comes from the box as in a simple tile.
 constexpr int TILE_SIMPLE = 1 << 30;
-__host__ __device__ inline int tile_gid(const Tile &t) { return t.gid & (TILE_SIMPLE - 1); }
+constexpr int TILE_WRAP = 1 << 29;
+__host__ __device__ inline int tile_gid(const Tile &t) { return t.gid & (TILE_WRAP - 1); }
 __host__ __device__ inline bool tile_simple(const Tile &t) { return (t.gid & TILE_SIMPLE) != 0; }
+__host__ __device__ inline bool tile_wrap(const Tile &t) { return (t.gid & TILE_WRAP) != 0; }
 
 // lattice (setupVars, cpuLBM.cpp:376-388) in units of c, its signs, and the
 // reflection maps of mirIndex (cpuLBM.cpp:1147-1169)

@@ -324,17 +324,31 @@ void prepare_sample(const HostSample &h, int prec, PreparedSample &out)
 
 // Tiles of one sample, each flagged simple when it and its 3-node halo lie
 // inside the domain and hold only plain fluid nodes.
-void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, int sample, std::vector<Tile> &out)
+void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, int sflags, int sample,
+               std::vector<Tile> &out)
 {
+    const bool px = (sflags & SF_PERX) != 0, py = (sflags & SF_PERY) != 0;
     for (int y0 = 0; y0 < ny; y0 += ty)
         for (int x0 = 0; x0 < nx; x0 += tx) {
             int gid = (int)out.size();
-            if (x0 >= 3 && y0 >= 3 && x0 + tx + 3 <= nx && y0 + ty + 3 <= ny) {
+            const bool in_x = x0 >= 3 && x0 + tx + 3 <= nx, in_y = y0 >= 3 && y0 + ty + 3 <= ny;
+            if (in_x && in_y) {
                 bool simple = true;
                 for (int y = y0 - 3; y < y0 + ty + 3 && simple; ++y)
                     for (int x = x0 - 3; x < x0 + tx + 3; ++x)
                         if (flags[(long long)y * pitch + x] != 0) { simple = false; break; }
                 if (simple) gid |= TILE_SIMPLE;
+            } else if ((in_x || px) && (in_y || py) && x0 + tx <= nx && y0 + ty <= ny) {
+                // a full tile whose halo crosses a periodic edge: plain fluid
+                // everywhere in the halo (periodic images included), and no
+                // flag but the stencil-wraps bits
+                bool wrap = true;
+                for (int y = y0 - 3; y < y0 + ty + 3 && wrap; ++y)
+                    for (int x = x0 - 3; x < x0 + tx + 3; ++x) {
+                        const int xw = ((x % nx) + nx) % nx, yw = ((y % ny) + ny) % ny;
+                        if (flags[(long long)yw * pitch + xw] & ~(NF_WRPX | NF_WRPY)) { wrap = false; break; }
+                    }
+                if (wrap) gid |= TILE_WRAP;
             }
             out.push_back(Tile{sample, x0, y0, gid});
         }
@@ -380,8 +394,9 @@ struct lbm_batch {
     std::vector<HostSample> hs;
     std::vector<SampleParams> sp;
     std::vector<Tile> tiles_all, tiles_rk3;
-    std::vector<Tile> tiles_by_rk[4], tiles_flux[4];  // by RKMETHOD: sample order, simple first
-    int ns_by_rk[4] = {0, 0, 0, 0}, ns_rk3 = 0;      // leading simple tiles of tiles_flux, tiles_rk3
+    std::vector<Tile> tiles_by_rk[4], tiles_flux[4];  // by RKMETHOD: sample order; by kind
+    // leading simple tiles and the wrap tiles after them in tiles_flux, tiles_rk3
+    int ns_by_rk[4] = {0, 0, 0, 0}, nw_by_rk[4] = {0, 0, 0, 0}, ns_rk3 = 0, nw_rk3 = 0;
     std::vector<WallNode> walls_all, walls_rk3;
     std::vector<int> tile_first, tile_count;
     long long total_state = 0, total_nodes = 0, lattice_nodes = 0;
@@ -425,7 +440,7 @@ struct lbm_batch {
             const HostSample &h = hs[k];
             SampleParams &p = sp[k];
             p.first_tile = (int)tiles_all.size();
-            cut_tiles(flags_host.data() + p.node_off, p.pitch, h.nx, h.ny, tx, ty, (int)k, tiles_all);
+            cut_tiles(flags_host.data() + p.node_off, p.pitch, h.nx, h.ny, tx, ty, p.flags, (int)k, tiles_all);
             p.ntile = (int)tiles_all.size() - p.first_tile;
             for (int t = p.first_tile; t < p.first_tile + p.ntile; ++t) {
                 tiles_by_rk[h.rk].push_back(tiles_all[t]);
@@ -434,13 +449,13 @@ struct lbm_batch {
             tile_first.push_back(p.first_tile);
             tile_count.push_back(p.ntile);
         }
-        // the stencil phases take the tiles simple ones first (one kernel
-        // per kind); the pointwise phase keeps the sample order
+        // the stencil phases take the tiles by kind (one kernel per kind);
+        // the pointwise phase keeps the sample order
         for (int m = 0; m < 4; ++m) {
             tiles_flux[m] = tiles_by_rk[m];
-            ns_by_rk[m] = simple_first(tiles_flux[m]);
+            order_by_kind(tiles_flux[m], ns_by_rk[m], nw_by_rk[m]);
         }
-        ns_rk3 = simple_first(tiles_rk3);
+        order_by_kind(tiles_rk3, ns_rk3, nw_rk3);
     }
 
     void upload_tiles()
@@ -667,9 +682,11 @@ struct lbm_batch {
         StepLists l;
         for (int m = 0; m < 4; ++m) {
             l.pointwise[m] = TileRun{d_tiles_by_rk[m].p, (int)tiles_by_rk[m].size()};
-            split_runs(d_tiles_flux[m].p, (int)tiles_flux[m].size(), ns_by_rk[m], l.simple[m], l.general[m]);
+            split_runs(d_tiles_flux[m].p, (int)tiles_flux[m].size(), ns_by_rk[m], nw_by_rk[m], l.simple[m], l.wrap[m],
+                       l.general[m]);
         }
-        if (any_rk3) split_runs(d_tiles_rk3.p, (int)tiles_rk3.size(), ns_rk3, l.rk3_simple, l.rk3_general);
+        if (any_rk3)
+            split_runs(d_tiles_rk3.p, (int)tiles_rk3.size(), ns_rk3, nw_rk3, l.rk3_simple, l.rk3_wrap, l.rk3_general);
         l.walls_all = d_walls_all.p;
         l.n_walls_all = (int)walls_all.size();
         l.walls_rk3 = d_walls_rk3.p;

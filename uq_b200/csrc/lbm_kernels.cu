@@ -720,8 +720,9 @@ __device__ void wrap_fixup(TileCtx<S, C> &k, int g, S *boxes)
 // Group g of G directions: wait for its staged boxes, the face fluxes
 // (posFluxes/computeFlux, cpuLBM.cpp:1405-1500; solid nodes answer
 // wallFluxes' alpha |e| f, cpuLBM.cpp:1576-1586) and edge fluxes of each,
-// one barrier, refill the slot, then each direction's divergence.
-template <class S, class C, bool SIMPLE, int G, int FM>
+// one barrier, refill the slot, then each direction's divergence.  WRAP:
+// a wrap tile (simple code after the periodic images are copied in).
+template <class S, class C, bool SIMPLE, int G, int FM, bool WRAP = false>
 __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
 {
     constexpr int NST = GroupCfg<G>::NSTAGE;
@@ -736,7 +737,7 @@ __device__ __forceinline__ void dir_group(TileCtx<S, C> &k, const int g)
         atomicOr(k.status, STATUS_TIMEOUT);
     }
     const S *boxes = k.stg + (size_t)slot * 2 * G * k.pstride;
-    if (!SIMPLE && k.wrap_fix) {
+    if ((WRAP || !SIMPLE) && k.wrap_fix) {
         // k.wrap_fix is the same for the whole block
         wrap_fixup<G>(k, g, const_cast<S *>(boxes));
         __syncthreads();
@@ -817,7 +818,7 @@ __device__ __forceinline__ void group_divergence_c(TileCtx<S, C> &k)
 }
 
 // dir_group with the group fixed at compile time, then the next group
-template <class S, class C, int FM, int G, int g>
+template <class S, class C, int FM, int G, int g, bool WRAP = false>
 __device__ __forceinline__ void run_groups_c(TileCtx<S, C> &k)
 {
     if constexpr (g < GroupCfg<G>::NGROUP) {
@@ -829,6 +830,10 @@ __device__ __forceinline__ void run_groups_c(TileCtx<S, C> &k)
             atomicOr(k.status, STATUS_TIMEOUT);
         }
         const S *boxes = k.stg + (size_t)slot * 2 * G * k.pstride;
+        if constexpr (WRAP) {
+            wrap_fixup<G>(k, g, const_cast<S *>(boxes));
+            __syncthreads();
+        }
         int ring0 = 0;
         group_fluxes_c<S, C, FM, G, g, 0>(k, boxes, ring0);
         __syncthreads();
@@ -836,7 +841,7 @@ __device__ __forceinline__ void run_groups_c(TileCtx<S, C> &k)
         else if (flux_prefetch(sizeof(S)) && g == GroupCfg<G>::NGROUP - NST && k.tid == 0)
             issue_state_prefetch<G>(k, slot);
         group_divergence_c<S, C, G, g, 0>(k);
-        run_groups_c<S, C, FM, G, g + 1>(k);
+        run_groups_c<S, C, FM, G, g + 1, WRAP>(k);
     }
 }
 
@@ -855,8 +860,10 @@ size_t flux_smem_bytes_t(size_t es, int tx, int ty)
 // 3 = RK1 update, 4 = EULER update, 5 = EULER_EQ update (buffer 2)
 // PATH (FluxPath): FLUX_SIMPLE / FLUX_GENERAL compile only the code of that
 // kind of tile (the two together are far smaller per kernel than one kernel
-// holding both, which the register allocation of the simple path needs); a
-// block given a tile of the other kind returns at once.
+// holding both, which the register allocation of the simple path needs);
+// FLUX_WRAP is the simple code with the periodic images copied into each
+// staged box before use.  A block given a tile of another kind returns at
+// once.
 // T16: the tile shape is the default 16 x 16, compiled in (box widths,
 // strides and the thread-to-node map become constants); otherwise read from
 // the arguments.
@@ -881,7 +888,8 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     __shared__ int s_timeout;
 
     const Tile t = a.tiles[blockIdx.x];
-    if (tile_simple(t) != (PATH == FLUX_SIMPLE)) return;
+    if ((tile_simple(t) ? FLUX_SIMPLE : tile_wrap(t) ? FLUX_WRAP : FLUX_GENERAL) != PATH) return;
+    constexpr bool WRAPT = PATH == FLUX_WRAP;
     const int tid = threadIdx.x;
     constexpr int PH = MODE == 2 ? 2 : 1;
     const CUtensorMap *map = a.tmaps + MAPS_PER_SAMPLE * t.sample + (PH == 1 ? 0 : 1);
@@ -932,24 +940,24 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     const int type = k.flag & NF_TYPE;
     sD[tid] = C(0);          // direction 0 streams nothing
     sD[NQ * NT + tid] = C(0);
-    if (PATH == FLUX_SIMPLE) {
+    if (PATH != FLUX_GENERAL) {
         // simple tiles: the flux scheme fixed at compile time (smaller hot
         // code); for narrow-range WENO5, the common case, in FP32 and in the
         // FP64 final phase also every direction (the other instances lose
         // more to their larger code than they gain)
         if (sp.fm && sizeof(S) == 4 && sp.wide) {
 #pragma unroll 1
-            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 2>(k, g);
+            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 2, WRAPT>(k, g);
         } else if (sp.fm) {
             if constexpr (G == 4 || MODE == 2) {
-                run_groups_c<S, C, 1, G, 0>(k);
+                run_groups_c<S, C, 1, G, 0, WRAPT>(k);
             } else {
 #pragma unroll 1
-                for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 1>(k, g);
+                for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 1, WRAPT>(k, g);
             }
         } else {
 #pragma unroll 1
-            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 0>(k, g);
+            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 0, WRAPT>(k, g);
         }
     } else {
 #pragma unroll 1
@@ -1308,8 +1316,9 @@ cudaError_t launch_phase(const KArgs<S> &a, int phase, int rk, const Tile *tiles
         if (!ntiles) return cudaSuccess;
         const size_t sm = flux_smem_bytes_t(sizeof(S), a.tx, a.ty);
         const int mode = phase == 2 ? 2 : (rk == 1 ? 1 : (rk == 0 ? 3 : (rk == 2 ? 4 : 5)));
-        if (path != FLUX_GENERAL) launch_flux<S, C, FLUX_SIMPLE>(mode, k, ntiles, NT, sm, st);
-        if (path != FLUX_SIMPLE) launch_flux<S, C, FLUX_GENERAL>(mode, k, ntiles, NT, sm, st);
+        if (path == FLUX_BOTH || path == FLUX_SIMPLE) launch_flux<S, C, FLUX_SIMPLE>(mode, k, ntiles, NT, sm, st);
+        if (path == FLUX_WRAP) launch_flux<S, C, FLUX_WRAP>(mode, k, ntiles, NT, sm, st);
+        if (path == FLUX_BOTH || path == FLUX_GENERAL) launch_flux<S, C, FLUX_GENERAL>(mode, k, ntiles, NT, sm, st);
     } else if (phase == 3 || phase == 4) {
         if (nwalls) k_wall<S, C><<<(nwalls + 127) / 128, 128, 0, st>>>(k, phase == 3 ? a.buf2 : a.buf3, walls, nwalls);
     }
@@ -1329,6 +1338,8 @@ cudaError_t prepare_kernels()
     UQ_FLUX_SMEM(4, FLUX_SIMPLE) UQ_FLUX_SMEM(5, FLUX_SIMPLE)
     UQ_FLUX_SMEM(1, FLUX_GENERAL) UQ_FLUX_SMEM(2, FLUX_GENERAL) UQ_FLUX_SMEM(3, FLUX_GENERAL)
     UQ_FLUX_SMEM(4, FLUX_GENERAL) UQ_FLUX_SMEM(5, FLUX_GENERAL)
+    UQ_FLUX_SMEM(1, FLUX_WRAP) UQ_FLUX_SMEM(2, FLUX_WRAP) UQ_FLUX_SMEM(3, FLUX_WRAP)
+    UQ_FLUX_SMEM(4, FLUX_WRAP) UQ_FLUX_SMEM(5, FLUX_WRAP)
 #undef UQ_FLUX_SMEM
 #undef UQ_FLUX_SMEM1
     return e;

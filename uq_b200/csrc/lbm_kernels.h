@@ -53,11 +53,11 @@ struct KArgs {
 #endif
 };
 
-// Which tiles a stencil-phase launch covers: FLUX_SIMPLE and FLUX_GENERAL
-// run the kernel compiled for that kind alone over a list holding only that
-// kind; FLUX_BOTH runs both kernels over a mixed list (each skips the
-// other kind's tiles).
-enum FluxPath { FLUX_BOTH = 0, FLUX_SIMPLE = 1, FLUX_GENERAL = 2 };
+// Which tiles a stencil-phase launch covers: FLUX_SIMPLE, FLUX_WRAP and
+// FLUX_GENERAL run the kernel compiled for that kind alone over a list
+// holding only that kind; FLUX_BOTH runs the simple and the general kernel
+// over a list of those two kinds (each skips the other kind's tiles).
+enum FluxPath { FLUX_BOTH = 0, FLUX_SIMPLE = 1, FLUX_GENERAL = 2, FLUX_WRAP = 3 };
 
 template <class S, class C>
 cudaError_t launch_phase(const KArgs<S> &a, int phase, int rk, const Tile *tiles, int ntiles, const WallNode *walls,

@@ -149,7 +149,9 @@ struct lbm_server {
     std::vector<SampleParams> sp;
     std::vector<Tile> tiles_all, tiles_rk3, tiles_by_rk[4];
     // stencil-phase lists: the simple tiles of every solve, then the others
-    std::vector<Tile> flux_by_rk[4], gen_rk3, gen_by_rk[4];
+    // stencil runs being built: simple tiles (flux_by_rk, tiles_rk3), wrap
+    // tiles and the rest, concatenated in that order
+    std::vector<Tile> flux_by_rk[4], gen_rk3, gen_by_rk[4], wrap_rk3, wrap_by_rk[4];
     std::vector<WallNode> walls_all, walls_rk3;
     std::vector<double> v_tdx, v_tdy, v_dx, v_dy, v_fref;
     std::vector<CUtensorMap> maps;
@@ -282,7 +284,7 @@ struct lbm_server {
         r->ny = h.ny;
         r->steps_total = h.nsteps;
         r->nodes = r->ps.p.plane;
-        cut_tiles(r->ps.flags.data(), r->ps.p.pitch, h.nx, h.ny, tx, ty, 0, r->tiles);
+        cut_tiles(r->ps.flags.data(), r->ps.p.pitch, h.nx, h.ny, tx, ty, r->ps.p.flags, 0, r->tiles);
         const long long n = (long long)h.nx * h.ny;
         r->fields.resize(4 * n);
         for (int x = 0; x < h.nx; ++x)
@@ -356,7 +358,9 @@ struct lbm_server {
         tiles_rk3.clear();
         for (auto &v : tiles_by_rk) v.clear();
         gen_rk3.clear();
+        wrap_rk3.clear();
         for (auto &v : gen_by_rk) v.clear();
+        for (auto &v : wrap_by_rk) v.clear();
         for (auto &v : flux_by_rk) v.clear();
         walls_all.clear();
         walls_rk3.clear();
@@ -379,12 +383,12 @@ struct lbm_server {
             for (const Tile &lt : r->tiles) {
                 Tile t = lt;
                 t.sample = (int)k;
-                t.gid = (int)tiles_all.size() | (lt.gid & TILE_SIMPLE);
+                t.gid = (int)tiles_all.size() | (lt.gid & (TILE_SIMPLE | TILE_WRAP));
                 tiles_all.push_back(t);
                 tiles_by_rk[p.rk].push_back(t);
-                const bool simple = tile_simple(t);
-                (simple ? flux_by_rk[p.rk] : gen_by_rk[p.rk]).push_back(t);
-                if (p.rk == 1) (simple ? tiles_rk3 : gen_rk3).push_back(t);
+                const bool simple = tile_simple(t), wrap = tile_wrap(t);
+                (simple ? flux_by_rk[p.rk] : wrap ? wrap_by_rk[p.rk] : gen_by_rk[p.rk]).push_back(t);
+                if (p.rk == 1) (simple ? tiles_rk3 : wrap ? wrap_rk3 : gen_rk3).push_back(t);
             }
             for (WallNode w : r->ps.walls) {
                 w.sample = (int)k;
@@ -400,11 +404,14 @@ struct lbm_server {
             sp.push_back(p);
             packed_nodes += (long long)r->nx * r->ny;
         }
-        int ns_by_rk[4], ns_rk3 = (int)tiles_rk3.size();
+        int ns_by_rk[4], nw_by_rk[4], ns_rk3 = (int)tiles_rk3.size(), nw_rk3 = (int)wrap_rk3.size();
         for (int m = 0; m < 4; ++m) {
             ns_by_rk[m] = (int)flux_by_rk[m].size();
+            nw_by_rk[m] = (int)wrap_by_rk[m].size();
+            flux_by_rk[m].insert(flux_by_rk[m].end(), wrap_by_rk[m].begin(), wrap_by_rk[m].end());
             flux_by_rk[m].insert(flux_by_rk[m].end(), gen_by_rk[m].begin(), gen_by_rk[m].end());
         }
+        tiles_rk3.insert(tiles_rk3.end(), wrap_rk3.begin(), wrap_rk3.end());
         tiles_rk3.insert(tiles_rk3.end(), gen_rk3.begin(), gen_rk3.end());
         d_sp.upload_keep(sp, stream);
         for (int m = 0; m < 4; ++m) {
@@ -423,30 +430,38 @@ struct lbm_server {
         lists = StepLists{};
         for (int m = 0; m < 4; ++m) {
             lists.pointwise[m] = TileRun{d_tiles_by_rk[m].p, (int)tiles_by_rk[m].size()};
-            split_runs(d_flux_by_rk[m].p, (int)flux_by_rk[m].size(), ns_by_rk[m], lists.simple[m], lists.general[m]);
+            split_runs(d_flux_by_rk[m].p, (int)flux_by_rk[m].size(), ns_by_rk[m], nw_by_rk[m], lists.simple[m],
+                       lists.wrap[m], lists.general[m]);
         }
-        split_runs(d_tiles_rk3.p, (int)tiles_rk3.size(), ns_rk3, lists.rk3_simple, lists.rk3_general);
+        split_runs(d_tiles_rk3.p, (int)tiles_rk3.size(), ns_rk3, nw_rk3, lists.rk3_simple, lists.rk3_wrap,
+                   lists.rk3_general);
         lists.walls_all = d_walls_all.p;
         lists.n_walls_all = (int)walls_all.size();
         lists.walls_rk3 = d_walls_rk3.p;
         lists.n_walls_rk3 = (int)walls_rk3.size();
         fast_lists = lists;
-        for (int m = 0; m < 4; ++m) fast_lists.pointwise[m].n = fast_lists.simple[m].n = fast_lists.general[m].n = 0;
-        fast_lists.rk3_simple.n = fast_lists.rk3_general.n = 0;
+        for (int m = 0; m < 4; ++m)
+            fast_lists.pointwise[m].n = fast_lists.simple[m].n = fast_lists.wrap[m].n = fast_lists.general[m].n = 0;
+        fast_lists.rk3_simple.n = fast_lists.rk3_wrap.n = fast_lists.rk3_general.n = 0;
         fast_lists.n_walls_all = fast_lists.n_walls_rk3 = 0;
         fast_nodes = 0;
         for (int k = 0; k < n_fast; ++k) {
             const Request *r = packed[k];
-            int ns = 0;
-            for (const Tile &t : r->tiles) ns += tile_simple(t) ? 1 : 0;
-            const int ng = (int)r->tiles.size() - ns, nw = (int)r->ps.walls.size();
+            int ns = 0, nwr = 0;
+            for (const Tile &t : r->tiles) {
+                ns += tile_simple(t) ? 1 : 0;
+                nwr += tile_wrap(t) ? 1 : 0;
+            }
+            const int ng = (int)r->tiles.size() - ns - nwr, nw = (int)r->ps.walls.size();
             const int m = r->ps.p.rk;
-            fast_lists.pointwise[m].n += ns + ng;
+            fast_lists.pointwise[m].n += ns + nwr + ng;
             fast_lists.simple[m].n += ns;
+            fast_lists.wrap[m].n += nwr;
             fast_lists.general[m].n += ng;
             fast_lists.n_walls_all += nw;
             if (m == 1) {
                 fast_lists.rk3_simple.n += ns;
+                fast_lists.rk3_wrap.n += nwr;
                 fast_lists.rk3_general.n += ng;
                 fast_lists.n_walls_rk3 += nw;
             }
