@@ -221,6 +221,17 @@ LBM_API lbm_status lbm_batch_set_dist(lbm_batch *b, int sample, const double *f,
  * (cpuLBM.cpp:846-875): the restart-from-fields / new-solve entry point. */
 LBM_API lbm_status lbm_batch_set_macro(lbm_batch *b, int sample, const double *rho, const double *ux,
                                        const double *uy, const double *T);
+/* Every sample's fields at once, for callers that move the whole ensemble
+ * (no counterpart in the reference, which runs one solve per process): the
+ * arrays hold the samples one after another in sample order, each in the
+ * [x*Ny + y] order of its own grid (sum over samples of Nx*Ny values per
+ * field).  One host<->device copy per field and one synchronisation, in
+ * place of one of each per sample.  Results are those of the per-sample
+ * calls. */
+LBM_API lbm_status lbm_batch_set_macro_all(lbm_batch *b, const double *rho, const double *ux, const double *uy,
+                                           const double *T);
+LBM_API lbm_status lbm_batch_get_macro_all(lbm_batch *b, double *rho, double *ux, double *uy, double *T,
+                                           double *p);
 /* Run n_steps steps outside any graph with CUDA events around every phase
  * and return the mean device milliseconds per step of each phase in
  * phase_ms[0..5]: pointwise stages, walls of buffer 2, stencil phase 1,

@@ -741,6 +741,67 @@ struct lbm_batch {
                                        reinterpret_cast<float *>(buf3.p), scratch.p, nflags.p, d_fref.p, n, stream));
     }
 
+    // all samples' fields in one device buffer (5 fields x lattice nodes,
+    // made on first use): per field one copy to or from the host
+    DevBuf<double> all_fields;
+    std::vector<long long> lattice_off;  // per sample: first value in the concatenated fields
+
+    void ensure_all_fields()
+    {
+        if (lattice_off.empty()) {
+            long long off = 0;
+            for (const HostSample &h : hs) {
+                lattice_off.push_back(off);
+                off += (long long)h.nx * h.ny;
+            }
+        }
+        if (all_fields.n < (size_t)(5 * lattice_nodes)) all_fields.alloc(5 * lattice_nodes);
+    }
+
+    void set_macro_all(const double *rho, const double *ux, const double *uy, const double *T)
+    {
+        ensure_all_fields();
+        const double *src[4] = {rho, ux, uy, T};
+        for (int k = 0; k < 4; ++k)
+            CU(cudaMemcpyAsync(all_fields.p + k * lattice_nodes, src[k], lattice_nodes * sizeof(double),
+                               cudaMemcpyHostToDevice, stream));
+        for (size_t s = 0; s < hs.size(); ++s) {
+            const long long n = (long long)hs[s].nx * hs[s].ny;
+            // the four fields of sample s, each n values, lattice_nodes apart
+            double *f0 = all_fields.p + lattice_off[s];
+            if (prec == LBM_PREC_F64)
+                CU(launch_set_macro_strided<double>(d_sp.p, (int)s, reinterpret_cast<double *>(state.p),
+                                                    reinterpret_cast<double *>(buf2.p),
+                                                    reinterpret_cast<double *>(buf3.p), f0, lattice_nodes, nflags.p,
+                                                    d_fref.p, n, stream));
+            else
+                CU(launch_set_macro_strided<float>(d_sp.p, (int)s, reinterpret_cast<float *>(state.p),
+                                                   reinterpret_cast<float *>(buf2.p), reinterpret_cast<float *>(buf3.p),
+                                                   f0, lattice_nodes, nflags.p, d_fref.p, n, stream));
+        }
+    }
+
+    void get_macro_all(double *rho, double *ux, double *uy, double *T, double *p)
+    {
+        ensure_all_fields();
+        for (size_t s = 0; s < hs.size(); ++s) {
+            const long long n = (long long)hs[s].nx * hs[s].ny;
+            double *out = all_fields.p + lattice_off[s];
+            if (prec == LBM_PREC_F64)
+                CU(launch_macro_out_strided<double>(d_sp.p, (int)s, reinterpret_cast<double *>(state.p), out,
+                                                    lattice_nodes, n, stream));
+            else
+                CU(launch_macro_out_strided<float>(d_sp.p, (int)s, reinterpret_cast<float *>(state.p), out,
+                                                   lattice_nodes, n, stream));
+        }
+        double *dst[5] = {rho, ux, uy, T, p};
+        for (int k = 0; k < 5; ++k)
+            if (dst[k])
+                CU(cudaMemcpyAsync(dst[k], all_fields.p + k * lattice_nodes, lattice_nodes * sizeof(double),
+                                   cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+    }
+
     void enqueue_step(int want_res)
     {
         if (prec == LBM_PREC_F64) enqueue_step_t<double, double>(want_res);
@@ -1174,6 +1235,25 @@ lbm_status lbm_batch_set_macro(lbm_batch *b, int sample, const double *rho, cons
     if (!b || !rho || !ux || !uy || !T || sample < 0 || sample >= (int)b->hs.size())
         throw LbmError(LBM_ERR_INVALID, "bad argument");
     b->set_macro(sample, rho, ux, uy, T);
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_batch_set_macro_all(lbm_batch *b, const double *rho, const double *ux, const double *uy,
+                                   const double *T)
+{
+    API_BEGIN
+    if (!b || !rho || !ux || !uy || !T) throw LbmError(LBM_ERR_INVALID, "bad argument");
+    b->set_macro_all(rho, ux, uy, T);
+    return LBM_OK;
+    API_END
+}
+
+lbm_status lbm_batch_get_macro_all(lbm_batch *b, double *rho, double *ux, double *uy, double *T, double *p)
+{
+    API_BEGIN
+    if (!b) throw LbmError(LBM_ERR_INVALID, "bad argument");
+    b->get_macro_all(rho, ux, uy, T, p);
     return LBM_OK;
     API_END
 }

@@ -1199,9 +1199,9 @@ __global__ void k_residual(const SampleParams *samples, int nsamples, const doub
 
 // ------------------------------------------------------------ boundary I/O
 // macroPropShort for every node of one sample, written in the reference's
-// [x*Ny + y] order.
+// [x*Ny + y] order: rho, ux, uy, T, p, each `stride` values apart.
 template <class S>
-__global__ void k_macro_out(const SampleParams *samples, int s, const S *state, double *out)
+__global__ void k_macro_out(const SampleParams *samples, int s, const S *state, double *out, long long stride)
 {
     const SampleParams sp = samples[s];
     const long long n = (long long)sp.nx * sp.ny;
@@ -1209,10 +1209,10 @@ __global__ void k_macro_out(const SampleParams *samples, int s, const S *state, 
         const int y = (int)(k % sp.ny), x = (int)(k / sp.ny);
         const Macro m = node_macro_at(state + sp.state_off, sp, (long long)y * sp.pitch + x);
         out[k] = m.rho;
-        out[n + k] = m.ux;
-        out[2 * n + k] = m.uy;
-        out[3 * n + k] = m.T;
-        out[4 * n + k] = m.p;
+        out[stride + k] = m.ux;
+        out[2 * stride + k] = m.uy;
+        out[3 * stride + k] = m.T;
+        out[4 * stride + k] = m.p;
     }
 }
 
@@ -1247,10 +1247,11 @@ __global__ void k_dist_io(const SampleParams *samples, int s, S *state, S *buf2,
     }
 }
 
-// f, h = equilibria of per-node fields given in [x*Ny + y] order (FP64)
+// f, h = equilibria of per-node fields given in [x*Ny + y] order (FP64):
+// rho, ux, uy, T, each `stride` values apart
 template <class S>
 __global__ void k_set_macro(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, const double *fields,
-                            const uint8_t *nflags, const double *fref)
+                            long long stride, const uint8_t *nflags, const double *fref)
 {
     const double *fr = fref + NPL * s;
     const SampleParams sp = samples[s];
@@ -1259,18 +1260,33 @@ __global__ void k_set_macro(const SampleParams *samples, int s, S *state, S *buf
         const int y = (int)(k % sp.ny), x = (int)(k / sp.ny);
         const long long o = (long long)y * sp.pitch + x;
         const bool fixed = (nflags[sp.node_off + o] & NF_TYPE) != 0;
-        init_node<S>(fields[k], fields[n + k], fields[2 * n + k], fields[3 * n + k], sp, fr, state, buf2, buf3, o, fixed);
+        init_node<S>(fields[k], fields[stride + k], fields[2 * stride + k], fields[3 * stride + k], sp, fr, state, buf2,
+                     buf3, o, fixed);
     }
+}
+
+template <class S>
+cudaError_t launch_set_macro_strided(const SampleParams *samples, int s, S *state, S *buf2, S *buf3,
+                                     const double *fields, long long stride, const uint8_t *nflags, const double *fref,
+                                     long long nodes, cudaStream_t st)
+{
+    const int blocks = (int)std::min<long long>((nodes + 255) / 256, 4096);
+    k_set_macro<S><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(samples, s, state, buf2, buf3, fields, stride, nflags, fref);
+    return cudaGetLastError();
 }
 
 template <class S>
 cudaError_t launch_set_macro(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, const double *fields,
                              const uint8_t *nflags, const double *fref, long long nodes, cudaStream_t st)
 {
-    const int blocks = (int)std::min<long long>((nodes + 255) / 256, 4096);
-    k_set_macro<S><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(samples, s, state, buf2, buf3, fields, nflags, fref);
-    return cudaGetLastError();
+    return launch_set_macro_strided<S>(samples, s, state, buf2, buf3, fields, nodes, nflags, fref, nodes, st);
 }
+template cudaError_t launch_set_macro_strided<double>(const SampleParams *, int, double *, double *, double *,
+                                                      const double *, long long, const uint8_t *, const double *,
+                                                      long long, cudaStream_t);
+template cudaError_t launch_set_macro_strided<float>(const SampleParams *, int, float *, float *, float *,
+                                                     const double *, long long, const uint8_t *, const double *,
+                                                     long long, cudaStream_t);
 template cudaError_t launch_set_macro<double>(const SampleParams *, int, double *, double *, double *, const double *,
                                               const uint8_t *, const double *, long long, cudaStream_t);
 template cudaError_t launch_set_macro<float>(const SampleParams *, int, float *, float *, float *, const double *,
@@ -1356,12 +1372,19 @@ cudaError_t launch_init(const KArgs<S> &a, const double *rho, const double *ux, 
 }
 
 template <class S>
+cudaError_t launch_macro_out_strided(const SampleParams *samples, int s, const S *state, double *out,
+                                     long long stride, long long nodes, cudaStream_t st)
+{
+    const int blocks = (int)std::min<long long>((nodes + 255) / 256, 4096);
+    k_macro_out<S><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(samples, s, state, out, stride);
+    return cudaGetLastError();
+}
+
+template <class S>
 cudaError_t launch_macro_out(const SampleParams *samples, int s, const S *state, double *out, long long nodes,
                              cudaStream_t st)
 {
-    const int blocks = (int)std::min<long long>((nodes + 255) / 256, 4096);
-    k_macro_out<S><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(samples, s, state, out);
-    return cudaGetLastError();
+    return launch_macro_out_strided<S>(samples, s, state, out, nodes, nodes, st);
 }
 
 template <class S>
@@ -1415,6 +1438,10 @@ template cudaError_t launch_init<double>(const KArgs<double> &, const double *, 
                                          const double *, cudaStream_t);
 template cudaError_t launch_init<float>(const KArgs<float> &, const double *, const double *, const double *,
                                         const double *, cudaStream_t);
+template cudaError_t launch_macro_out_strided<double>(const SampleParams *, int, const double *, double *, long long,
+                                                      long long, cudaStream_t);
+template cudaError_t launch_macro_out_strided<float>(const SampleParams *, int, const float *, double *, long long,
+                                                     long long, cudaStream_t);
 template cudaError_t launch_macro_out<double>(const SampleParams *, int, const double *, double *, long long, cudaStream_t);
 template cudaError_t launch_macro_out<float>(const SampleParams *, int, const float *, double *, long long, cudaStream_t);
 template cudaError_t launch_dist_io<double>(const SampleParams *, int, double *, double *, double *, double *, int,

@@ -71,6 +71,15 @@ cudaError_t launch_init(const KArgs<S> &a, const double *rho, const double *ux, 
 template <class S>
 cudaError_t launch_macro_out(const SampleParams *samples, int s, const S *state, double *out, long long nodes,
                              cudaStream_t st);
+// the same with the fields `stride` values apart (several samples' fields
+// in one buffer)
+template <class S>
+cudaError_t launch_macro_out_strided(const SampleParams *samples, int s, const S *state, double *out,
+                                     long long stride, long long nodes, cudaStream_t st);
+template <class S>
+cudaError_t launch_set_macro_strided(const SampleParams *samples, int s, S *state, S *buf2, S *buf3,
+                                     const double *fields, long long stride, const uint8_t *nflags, const double *fref,
+                                     long long nodes, cudaStream_t st);
 template <class S>
 cudaError_t launch_dist_io(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, double *aos, int to_aos,
                            const uint8_t *nflags, const double *fref, long long nodes, cudaStream_t st);

@@ -110,6 +110,8 @@ SIGNATURES = {
     "lbm_batch_get_dist": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     "lbm_batch_set_dist": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     "lbm_batch_set_macro": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]),
+    "lbm_batch_set_macro_all": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    "lbm_batch_get_macro_all": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     "lbm_batch_profile": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int]),
     "lbm_batch_launches_per_step": (C.c_int, [C.c_void_p, C.c_int]),
     "lbm_batch_autotune": (C.c_int, [C.c_void_p, _ip, C.c_int, C.c_int, _ip, _dp]),

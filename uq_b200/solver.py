@@ -324,6 +324,40 @@ class Batch:
         N.check(N.lib().lbm_batch_get_macro(self._h, int(s), c(rho, _dp), c(ux, _dp), c(uy, _dp), c(T, _dp),
                                             c(p, _dp)), "lbm_batch_get_macro")
 
+    def set_macro_all_ptr(self, rho, ux, uy, T):
+        """Every sample's fields at once from host buffers given as raw
+        addresses (samples one after another, each [x*Ny + y]); asynchronous
+        on the batch's stream."""
+        c = C.cast
+        N.check(N.lib().lbm_batch_set_macro_all(self._h, c(rho, _dp), c(ux, _dp), c(uy, _dp), c(T, _dp)),
+                "lbm_batch_set_macro_all")
+
+    def macro_all_ptr(self, rho, ux, uy, T, p):
+        """Every sample's fields at once into host buffers given as raw
+        addresses (same layout as set_macro_all_ptr)."""
+        c = C.cast
+        N.check(N.lib().lbm_batch_get_macro_all(self._h, c(rho, _dp), c(ux, _dp), c(uy, _dp), c(T, _dp), c(p, _dp)),
+                "lbm_batch_get_macro_all")
+
+    def macro_all(self):
+        """[macro(s) for every sample], through one bulk copy."""
+        n = sum(nx * ny for nx, ny in self.shapes)
+        out = {k: np.empty(n) for k in ("rho", "ux", "uy", "T", "p")}
+        N.check(N.lib().lbm_batch_get_macro_all(self._h, *[_d(out[k]) for k in ("rho", "ux", "uy", "T", "p")]),
+                "lbm_batch_get_macro_all")
+        res, off = [], 0
+        for nx, ny in self.shapes:
+            res.append({k: v[off:off + nx * ny].reshape(nx, ny) for k, v in out.items()})
+            off += nx * ny
+        return res
+
+    def set_macro_all(self, fields):
+        """fields: one dict (rho, ux, uy, T as [Nx, Ny]) per sample."""
+        arrs = [np.ascontiguousarray(np.concatenate([np.asarray(f[k], dtype=np.float64).reshape(-1) for f in fields]))
+                for k in ("rho", "ux", "uy", "T")]
+        N.check(N.lib().lbm_batch_set_macro_all(self._h, *[_d(a) for a in arrs]), "lbm_batch_set_macro_all")
+        self.status()  # synchronises: the host arrays may be released after return
+
     def set_macro(self, s, rho, ux, uy, T):
         arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (rho, ux, uy, T)]
         N.check(N.lib().lbm_batch_set_macro(self._h, int(s), *[_d(a) for a in arrs]), "lbm_batch_set_macro")
