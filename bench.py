@@ -358,6 +358,16 @@ def config_probes(seed=99, plate_steps=50):
     mlups = b.nodes * plate_steps / (ms * 1e3)
     st_end = b.status()
     b.close()
+    long_run = {}
+    if plate_steps >= 1000:
+        # the configured length: which plates complete, in FP32 and in FP64
+        b = Batch(plates, "f64")
+        ms64 = _timed_steps(b, plate_steps)
+        st64 = b.status()
+        b.close()
+        long_run = {"per_plate": [{"mach": m, "tau": t, "status_f32": int(a), "status_f64": int(c)}
+                                  for (m, t), a, c in zip(draws, st_end, st64)],
+                    "mlups_f64": sum(pl["bnd"].size for pl in plates) * plate_steps / (ms64 * 1e3)}
     b32, b64 = Batch(plates, "f32"), Batch(plates, "f64")
     b32.step(10)
     b64.step(10)
@@ -370,6 +380,7 @@ def config_probes(seed=99, plate_steps=50):
     b64.close()
     out["flat_plate_16x2048x512_weno5_rk3"] = {
         "mlups_f32": mlups, "steps_timed": plate_steps, "status_ok_after_timed_steps": int((st_end == 0).sum()),
+        **long_run,
         "f32_vs_f64_l2_max_10_steps": worst}
     return out
 

@@ -26,12 +26,12 @@ def test_profile_and_launch_count(cuda_device):
     b = Batch([W.couette(nx=64, ny=48, steps=4, seed=1)], "f32")
     ms = b.profile(2)
     assert ms.shape == (6,) and (ms[:5] >= 0).all() and ms[2] > 0
-    # 4 x 3 tiles of 16 x 16: in the middle row two simple tiles and, at the
-    # periodic edges, two wrap tiles; the rest touch the walls.  Pointwise,
-    # walls, stencil 1 (simple, wrap and general kernels), walls, stencil 2
-    # (all three), + residual
-    assert b.launches_per_step(False) == 9
-    assert b.launches_per_step(True) == 10
+    # 4 x 3 tiles of 16 x 16: the middle row is simple (the two at the
+    # periodic x edges read the ghost columns); the rest touch the walls.
+    # Pointwise, ghost columns of buffer 2, walls, stencil 1 (simple and
+    # general kernels), walls, stencil 2 (both), + residual
+    assert b.launches_per_step(False) == 8
+    assert b.launches_per_step(True) == 9
 
 
 def test_tile_shape_does_not_change_results(cuda_device):
@@ -64,15 +64,20 @@ def test_autotune_keeps_state_and_results(cuda_device):
 
 def test_wrap_tiles_match_oracle(cuda_device):
     """Tiles at periodic edges whose halo holds only plain fluid run the
-    simple-tile code on a staged box completed with the periodic images:
-    periodic in x (Couette) and in both axes (a smooth random state), FP64
-    against the oracle and FP32 within the mixed-path tolerance."""
+    simple-tile code: across an x edge the staged box reads the sample's
+    ghost columns, across a y edge (wrap tiles) the periodic images are
+    copied into it.  Periodic in x (Couette) and in both axes (a random
+    state), FP64 against the oracle and FP32 within the mixed-path
+    tolerance."""
     from oracle import oracle as O
 
     cases = [W.couette(nx=64, ny=48, steps=6, seed=5),
              W.random_state(64, 48, seed=6, bc="periodic", du=0.01, drho=0.01, dT=0.01, steps=6)]
     b = Batch(cases, "f64")
-    assert b.launches_per_step(False) == 9  # a wrap run in each stencil phase
+    # simple, wrap (the random state's tiles at its y edges) and general
+    # (Couette's wall rows) runs in each stencil phase, and buffer 2's
+    # ghost columns
+    assert b.launches_per_step(False) == 10
     b.step(6)
     b32 = Batch(cases, "f32")
     b32.step(6)

@@ -43,9 +43,17 @@ def _alone(case, precision):
     return st, out
 
 
+def _case_slots(c):
+    """Node slots a solve takes in the arena: ny rows of its pitch, which
+    holds 4 ghost columns on each side when the solve is periodic in x."""
+    nx, ny = c["bnd"].shape
+    ghosts = 8 if c.get("periodicX") and nx >= 8 else 0
+    return ny * (-(-(nx + ghosts) // 32) * 32)
+
+
 def _arena_for(cases, precision, resident):
     """An arena that holds about `resident` of the largest solves."""
-    slots = max(c["bnd"].shape[1] * ((c["bnd"].shape[0] + 31) // 32 * 32) for c in cases)
+    slots = max(_case_slots(c) for c in cases)
     return int(resident * slots * BYTES_PER_NODE[precision]) + 4096
 
 
@@ -162,14 +170,15 @@ def test_cancel_release_and_errors(cuda_device):
 
 
 def test_fragmented_arena_is_compacted(cuda_device):
-    # three 64 x 64 solves (4096 node slots each) fill an arena of ~3.6 of
+    # three 64 x 64 solves (64 x 96 node slots each) fill an arena of ~3.6 of
     # them; the middle one finishes first and leaves a hole too small for a
-    # 96 x 64 solve (6144 slots), although the free total is large enough
+    # 96 x 64 solve (64 x 128 slots), although the free total is large enough
     a = W.couette(nx=64, ny=64, steps=3000, seed=11)
     b = W.couette(nx=64, ny=64, steps=5, seed=12)
     c = W.couette(nx=64, ny=64, steps=3000, seed=13, fmethod=0)
     d = W.couette(nx=96, ny=64, steps=20, seed=14, rkmethod=0)
-    slots = 4096
+    slots, slots_d = _case_slots(a), _case_slots(d)
+    assert slots_d > 0.6 * slots  # the hole b leaves, and the free end, are each too small for d
     srv = Server(precision="f32", arena_bytes=int(3.6 * slots * BYTES_PER_NODE["f32"]), use_graph=False)
     ids = [srv.submit(a), srv.submit(b), srv.submit(c)]
     assert srv.wait(ids[1], timeout=120.0)

@@ -89,7 +89,7 @@ void prepare_sample(const HostSample &h, int prec, PreparedSample &out);
 // append the tx x ty tiles of one sample (flags in pitch layout, sample
 // flags sflags for its periodic axes) with the given sample index; gid
 // numbers continue from out.size()
-void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, int sflags, int sample,
+void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, int sflags, int gx, int sample,
                std::vector<Tile> &out);
 // TMA descriptors of one sample (MAPS_PER_SAMPLE of them): stage buffers 2
 // and 3 with the stencil halo box, and the state with the tile's own box
@@ -115,6 +115,11 @@ struct StepLists {
     TileRun rk3_simple, rk3_wrap, rk3_general;      // RK3 tiles (final stencil phase)
     const WallNode *walls_all = nullptr, *walls_rk3 = nullptr;
     int n_walls_all = 0, n_walls_rk3 = 0;
+    // the samples, for copying buffer 2's ghost columns (SampleParams::gx)
+    // after the pointwise phase
+    const SampleParams *samples = nullptr;
+    int nsamples = 0;
+    bool any_ghost = false;
 };
 
 // A device list of n tiles whose first ns are simple and next nw wrap
@@ -158,12 +163,13 @@ void enqueue_step_phases(const KArgs<S> &a, const StepLists &l, cudaStream_t st,
     if (ev) CU(cudaEventRecord(ev[0], st));
     for (int m = 0; m < 4; ++m)
         if (l.pointwise[m].n) CU((launch_phase<S, C>(a, 0, m, l.pointwise[m].p, l.pointwise[m].n, nullptr, 0, st)));
+    if (l.any_ghost) CU(launch_fill_ghosts<S>(l.samples, 0, l.nsamples, a.buf2, nullptr, st));
     if (ev) CU(cudaEventRecord(ev[1], st));
     CU((launch_phase<S, C>(a, 3, 0, nullptr, 0, l.walls_all, l.n_walls_all, st)));
     if (ev) CU(cudaEventRecord(ev[2], st));
     for (int m = 0; m < 4; ++m) stencil_runs<S, C>(a, 1, m, l.simple[m], l.wrap[m], l.general[m], st);
-    if (ev) CU(cudaEventRecord(ev[3], st));
     const bool rk3 = l.rk3_simple.n || l.rk3_wrap.n || l.rk3_general.n;
+    if (ev) CU(cudaEventRecord(ev[3], st));
     if (rk3) CU((launch_phase<S, C>(a, 4, 1, nullptr, 0, l.walls_rk3, l.n_walls_rk3, st)));
     if (ev) CU(cudaEventRecord(ev[4], st));
     if (rk3) stencil_runs<S, C>(a, 2, 1, l.rk3_simple, l.rk3_wrap, l.rk3_general, st);
@@ -172,7 +178,7 @@ void enqueue_step_phases(const KArgs<S> &a, const StepLists &l, cudaStream_t st,
 
 inline int step_launches(const StepLists &l)
 {
-    int n = 0;
+    int n = l.any_ghost ? 1 : 0;
     for (int m = 0; m < 4; ++m)
         n += (l.pointwise[m].n ? 1 : 0) + (l.simple[m].n ? 1 : 0) + (l.wrap[m].n ? 1 : 0) + (l.general[m].n ? 1 : 0);
     n += l.n_walls_all ? 1 : 0;

@@ -45,11 +45,23 @@ struct SampleParams {
     double rho0, T0n, shref;  // T0n = T0 / Tc
     double inv_mu, two_over_bR;
     int wide;  // FP32 WENO5 weights in the range-safe form (see weno5)
+    // ghost columns of the stage buffers (0 or GHOST_X): x-periodic samples
+    // keep, left and right of every row of buffers 2 and 3, the periodic
+    // images of the gx columns at the other edge, so the staged halo boxes
+    // of tiles at those edges load them as they load any interior node.
+    // Rows stay aligned (pitch >= nx + 2 gx, a multiple of 32): the right
+    // ghosts follow the row, the left ones are the last gx elements of the
+    // row before (the sample's region starts GHOST_SLACK elements before
+    // plane 0 for the first row's).  The per-node arrays have no ghosts.
+    int gx;
     // viscosity law (codeCL.py:986-990): 0 constant mu, 1 VHS, 2 Sutherland;
     // mu(T) = mu (T/visc_T)^visc_exp [(visc_T + visc_S)/(T + visc_S)]
     int visc;
     double visc_exp, visc_S, visc_T;
 };
+
+constexpr int GHOST_X = 4;       // = the staged box's x halo
+constexpr int GHOST_SLACK = 32;  // state elements before plane 0 of a sample with ghosts (keeps it aligned)
 
 struct Tile {
     int sample;

@@ -223,7 +223,9 @@ void prepare_sample(const HostSample &h, int prec, PreparedSample &out)
     p = SampleParams{};
     p.nx = h.nx;
     p.ny = h.ny;
-    p.pitch = round_up(h.nx, 32);
+    // x-periodic samples wide enough for their images keep ghost columns
+    p.gx = (h.flags & SF_PERX) && h.nx >= 2 * GHOST_X ? GHOST_X : 0;
+    p.pitch = round_up(h.nx + 2 * p.gx, 32);
     p.flags = h.flags;
     p.rk = h.rk;
     p.fm = h.fm;
@@ -324,7 +326,7 @@ void prepare_sample(const HostSample &h, int prec, PreparedSample &out)
 
 // Tiles of one sample, each flagged simple when it and its 3-node halo lie
 // inside the domain and hold only plain fluid nodes.
-void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, int sflags, int sample,
+void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, int sflags, int gx, int sample,
                std::vector<Tile> &out)
 {
     const bool px = (sflags & SF_PERX) != 0, py = (sflags & SF_PERY) != 0;
@@ -348,7 +350,9 @@ void cut_tiles(const uint8_t *flags, int pitch, int nx, int ny, int tx, int ty, 
                         const int xw = ((x % nx) + nx) % nx, yw = ((y % ny) + ny) % ny;
                         if (flags[(long long)yw * pitch + xw] & ~(NF_WRPX | NF_WRPY)) { wrap = false; break; }
                     }
-                if (wrap) gid |= TILE_WRAP;
+                // crossing only the x edges of a sample with ghost columns,
+                // the staged box needs nothing more: a simple tile
+                if (wrap) gid |= gx && in_y ? TILE_SIMPLE : TILE_WRAP;
             }
             out.push_back(Tile{sample, x0, y0, gid});
         }
@@ -364,8 +368,11 @@ void encode_stage_maps(int prec, const SampleParams &p, unsigned char *state, un
     auto enc = tensor_map_encoder();
     const size_t es = prec == LBM_PREC_F64 ? 8 : 4;
     for (int b = 0; b < MAPS_PER_SAMPLE; ++b) {
-        unsigned char *base = (b == 0 ? buf2 : b == 1 ? buf3 : state) + (size_t)p.state_off * es;
-        cuuint64_t dims[3] = {(cuuint64_t)p.nx, (cuuint64_t)p.ny, (cuuint64_t)NPL};
+        // with ghost columns the tensor starts at the left ghosts and spans
+        // the pitch (boxes at the x edges then read the images); else it is
+        // the domain and boxes read zeros beyond it
+        unsigned char *base = (b == 0 ? buf2 : b == 1 ? buf3 : state) + (size_t)(p.state_off - p.gx) * es;
+        cuuint64_t dims[3] = {(cuuint64_t)(p.gx ? p.pitch : p.nx), (cuuint64_t)p.ny, (cuuint64_t)NPL};
         cuuint64_t strides[2] = {(cuuint64_t)p.pitch * es, (cuuint64_t)p.plane * es};
         cuuint32_t halo[3] = {(cuuint32_t)(tx + 8), (cuuint32_t)(ty + 6), 1};
         cuuint32_t own[3] = {(cuuint32_t)tx, (cuuint32_t)ty, (cuuint32_t)PREFETCH_PLANES};
@@ -401,7 +408,7 @@ struct lbm_batch {
     std::vector<int> tile_first, tile_count;
     long long total_state = 0, total_nodes = 0, lattice_nodes = 0;
     size_t max_nodes = 0;
-    bool any_rk3 = false, any_other = false;
+    bool any_rk3 = false, any_other = false, any_ghost = false;
 
     DevBuf<unsigned char> state, buf2, buf3, alpha;  // typed by precision
     DevBuf<uint8_t> nflags;
@@ -440,7 +447,7 @@ struct lbm_batch {
             const HostSample &h = hs[k];
             SampleParams &p = sp[k];
             p.first_tile = (int)tiles_all.size();
-            cut_tiles(flags_host.data() + p.node_off, p.pitch, h.nx, h.ny, tx, ty, p.flags, (int)k, tiles_all);
+            cut_tiles(flags_host.data() + p.node_off, p.pitch, h.nx, h.ny, tx, ty, p.flags, p.gx, (int)k, tiles_all);
             p.ntile = (int)tiles_all.size() - p.first_tile;
             for (int t = p.first_tile; t < p.first_tile + p.ntile; ++t) {
                 tiles_by_rk[h.rk].push_back(tiles_all[t]);
@@ -593,7 +600,7 @@ struct lbm_batch {
             const HostSample &h = hs[k];
             prepare_sample(h, prec, ps);
             SampleParams p = ps.p;
-            p.state_off = state_off;
+            p.state_off = state_off + (p.gx ? GHOST_SLACK : 0);  // the first row's left ghosts before it
             p.node_off = node_off;
             p.xoff = (int)v_tdx.size();
             p.yoff = (int)v_tdy.size();
@@ -608,11 +615,12 @@ struct lbm_batch {
                 walls_all.push_back(w);
                 if (h.rk == 1) walls_rk3.push_back(w);
             }
-            state_off += NPL * p.plane;
+            state_off += NPL * p.plane + (p.gx ? GHOST_SLACK : 0);
             node_off += p.plane;
             lattice_nodes += (long long)h.nx * h.ny;
             max_nodes = std::max(max_nodes, (size_t)h.nx * h.ny);
             if (h.rk == 1) any_rk3 = true; else any_other = true;
+            if (p.gx) any_ghost = true;
             sp.push_back(p);
         }
         total_state = state_off;
@@ -670,6 +678,7 @@ struct lbm_batch {
         dT.upload(T0, stream);
         if (prec == LBM_PREC_F64) CU(launch_init<double>(args<double>(0), dr.p, du.p, dv.p, dT.p, stream));
         else CU(launch_init<float>(args<float>(0), dr.p, du.p, dv.p, dT.p, stream));
+        fill_ghosts(0, n);
         CU(cudaStreamSynchronize(stream));
         // equilibrium failures during initialisation are not reported by the
         // reference (hasFailed is reset by runOne, cpuLBM.cpp:2288)
@@ -687,6 +696,9 @@ struct lbm_batch {
         }
         if (any_rk3)
             split_runs(d_tiles_rk3.p, (int)tiles_rk3.size(), ns_rk3, nw_rk3, l.rk3_simple, l.rk3_wrap, l.rk3_general);
+        l.samples = d_sp.p;
+        l.nsamples = (int)hs.size();
+        l.any_ghost = any_ghost;
         l.walls_all = d_walls_all.p;
         l.n_walls_all = (int)walls_all.size();
         l.walls_rk3 = d_walls_rk3.p;
@@ -727,6 +739,18 @@ struct lbm_batch {
         for (int p = 0; p < nph && p < 6; ++p) ms[p] = n ? acc[p] / n : 0.0;
     }
 
+    // the ghost columns of samples s0 .. s0 + ns - 1 after their state was set
+    void fill_ghosts(int s0, int ns)
+    {
+        if (!any_ghost) return;
+        if (prec == LBM_PREC_F64)
+            CU(launch_fill_ghosts<double>(d_sp.p, s0, ns, reinterpret_cast<double *>(buf2.p),
+                                          reinterpret_cast<double *>(buf3.p), stream));
+        else
+            CU(launch_fill_ghosts<float>(d_sp.p, s0, ns, reinterpret_cast<float *>(buf2.p),
+                                         reinterpret_cast<float *>(buf3.p), stream));
+    }
+
     void set_macro(int s, const double *rho, const double *ux, const double *uy, const double *T)
     {
         const long long n = (long long)hs[s].nx * hs[s].ny;
@@ -739,6 +763,7 @@ struct lbm_batch {
         else
             CU(launch_set_macro<float>(d_sp.p, s, reinterpret_cast<float *>(state.p), reinterpret_cast<float *>(buf2.p),
                                        reinterpret_cast<float *>(buf3.p), scratch.p, nflags.p, d_fref.p, n, stream));
+        fill_ghosts(s, 1);
     }
 
     // all samples' fields in one device buffer (5 fields x lattice nodes,
@@ -779,6 +804,7 @@ struct lbm_batch {
                                                    reinterpret_cast<float *>(buf2.p), reinterpret_cast<float *>(buf3.p),
                                                    f0, lattice_nodes, nflags.p, d_fref.p, n, stream));
         }
+        fill_ghosts(0, (int)hs.size());
     }
 
     void get_macro_all(double *rho, double *ux, double *uy, double *T, double *p)
@@ -888,6 +914,8 @@ struct lbm_batch {
         if (to_aos) {
             if (f) CU(cudaMemcpyAsync(f, scratch.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
             if (h) CU(cudaMemcpyAsync(h, scratch.p + n3, n3 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        } else {
+            fill_ghosts(s, 1);
         }
         CU(cudaStreamSynchronize(stream));
     }

@@ -29,6 +29,18 @@ __device__ __forceinline__ S *plane_ptr(S *base, const SampleParams &sp, int p)
     return base + sp.state_off + (long long)p * sp.plane;
 }
 
+// Ghost columns (SampleParams::gx): a node within gx of an x edge also
+// stores its stage-buffer values at its periodic image beyond the other
+// edge.  The offset of that image (0: none) for the node at x; RK3's stage
+// 3 stores each buffer-3 value at o and, when this is nonzero, at
+// o + offset too.  Buffer 2's ghosts are copied by k_fill_ghosts after the
+// pointwise phase (the pointwise kernel runs at 64 registers, where the
+// extra stores cost it spills).
+__device__ __forceinline__ int ghost_offset(const SampleParams &sp, int x)
+{
+    return sp.gx ? (x < sp.gx ? sp.nx : (x >= sp.nx - sp.gx ? -sp.nx : 0)) : 0;
+}
+
 // ------------------------------------------------------------------- init
 // initialiseFunctions (cpuLBM.cpp:846-875) for one node: f, h = equilibrium
 // of (rho, ux, uy, T), stored as deviations from the rest state; solid and
@@ -297,6 +309,7 @@ struct TileCtx {
     const CUtensorMap *map;
     const CUtensorMap *smap;  // the state, box of the tile's own nodes over PREFETCH_PLANES planes
     S *pref_h;                // where the h half of the prefetch lands
+    int gx;                   // the sample's ghost columns: TMA x coordinates are x + gx
     int *timed_out;  // shared flag
     bool wrap_fix;   // general tiles: the box crosses a periodic edge
     int *status;     // this sample's status word
@@ -316,8 +329,9 @@ __device__ __forceinline__ void issue_group_load(TileCtx<S, C> &k, int g, int sl
 #pragma unroll
     for (int m = 0; m < G; ++m) {
         const int dir = group_dir<G>(g, m);
-        tma_load_3d(dst + (size_t)(2 * m) * k.pstride, k.map, k.x0 - HALO_X, k.y0 - HALO_Y, dir, &k.bars[slot]);
-        tma_load_3d(dst + (size_t)(2 * m + 1) * k.pstride, k.map, k.x0 - HALO_X, k.y0 - HALO_Y, NQ + dir, &k.bars[slot]);
+        tma_load_3d(dst + (size_t)(2 * m) * k.pstride, k.map, k.x0 - HALO_X + k.gx, k.y0 - HALO_Y, dir, &k.bars[slot]);
+        tma_load_3d(dst + (size_t)(2 * m + 1) * k.pstride, k.map, k.x0 - HALO_X + k.gx, k.y0 - HALO_Y, NQ + dir,
+                    &k.bars[slot]);
     }
 }
 
@@ -332,8 +346,8 @@ __device__ __forceinline__ void issue_state_prefetch(TileCtx<S, C> &k, int slot)
     S *dst_f = const_cast<S *>(k.stg) + (size_t)slot * 2 * G * k.pstride;
     fence_proxy_async_smem();
     mbar_arrive_expect_tx(&k.bars[NST], 2 * bytes);
-    tma_load_3d(dst_f, k.smap, k.x0, k.y0, 0, &k.bars[NST]);
-    tma_load_3d(k.pref_h, k.smap, k.x0, k.y0, NQ, &k.bars[NST]);
+    tma_load_3d(dst_f, k.smap, k.x0 + k.gx, k.y0, 0, &k.bars[NST]);
+    tma_load_3d(k.pref_h, k.smap, k.x0 + k.gx, k.y0, NQ, &k.bars[NST]);
 }
 
 // reconstruction from the staged box (fast path; no solid, no domain edge
@@ -904,6 +918,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     if (tid == 0) {
         s_sp = a.samples[t.sample];
         s_timeout = 0;
+        k.gx = s_sp.gx;
         for (int b = 0; b < NST + (PREF ? 1 : 0); ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
         for (int g = 0; g < NST; ++g) issue_group_load<G>(k, g, g);
@@ -920,6 +935,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
     const C *alpha = a.template alpha_as<C>() + sp.node_off;
 
     k.sp = &sp;
+    k.gx = sp.gx;
     k.v = v;
     k.alpha = alpha;
     k.fref = a.fref + NPL * t.sample;
@@ -995,6 +1011,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             // RK3 stage 3 (cpuLBM.cpp:1928-1993) and the part of the update
             // (cpuLBM.cpp:1999-2042) that does not need the stage-3 fluxes
             final_phase = false;
+            const int gd = ghost_offset(sp, x);
             // stage-1 moments (= stage 2's) and the moments of f - div F(f2)
             // (macroProp3, cpuLBM.cpp:973-1032), both summed in FP64
             constexpr bool DEV = sizeof(S) == 4;
@@ -1061,6 +1078,10 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     const C acch = h - C(0.5) * Dh + hdt * ((e1h[k] - h2) * ith2 + (e3h[k] - h3) * ith3) - hdt * cpl;
                     b3[of] = (S)f3;
                     b3[oh] = (S)h3;
+                    if (gd) {
+                        b3[of + gd] = (S)f3;
+                        b3[oh + gd] = (S)h3;
+                    }
                     st[of] = (S)accf;
                     st[oh] = (S)acch;
                 }
@@ -1185,6 +1206,56 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
         }
     }
 }
+
+// Ghost columns (SampleParams::gx): block (s, p) copies, in every row of
+// plane p of sample s0 + s, the gx columns at each x edge of the domain to
+// the ghost columns beyond the other edge: x in [-gx, 0) gets x + nx, x in
+// [nx, nx + gx) gets x - nx.  The stepping kernels keep the ghosts of the
+// values they write; this refreshes them after the state is set from
+// outside (the fixed nodes' stage values change there).
+template <class S>
+__global__ void k_fill_ghosts(const SampleParams *samples, int s0, S *buf)
+{
+    const SampleParams sp = samples[s0 + blockIdx.x];
+    if (!sp.gx) return;  // else GHOST_X
+    constexpr int gx = GHOST_X, w = 2 * GHOST_X, U = 4;
+    const int nx = sp.nx, n = sp.ny * w, pitch = sp.pitch;
+    S *pl = buf + sp.state_off + (long long)blockIdx.y * sp.plane;
+    // element e: row e / w, ghost e % w (consecutive threads share a row);
+    // each thread loads U elements before it stores them
+    for (int base = threadIdx.x; base < n; base += U * blockDim.x) {
+        S v[U];
+        S *dst[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = base + u * blockDim.x;
+            dst[u] = nullptr;
+            if (e < n) {
+                const int y = e / w, c = e % w;
+                const int xg = c < gx ? c - gx : nx + (c - gx);  // the ghost
+                const int xs = c < gx ? xg + nx : c - gx;        // its image in the domain
+                S *row = pl + (long long)y * pitch;
+                v[u] = row[xs];
+                dst[u] = row + xg;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (dst[u]) *dst[u] = v[u];
+    }
+}
+
+template <class S>
+cudaError_t launch_fill_ghosts(const SampleParams *samples, int s0, int ns, S *buf2, S *buf3, cudaStream_t st)
+{
+    if (ns > 0) {
+        if (buf2) k_fill_ghosts<S><<<dim3(ns, NPL), 256, 0, st>>>(samples, s0, buf2);
+        if (buf3) k_fill_ghosts<S><<<dim3(ns, NPL), 256, 0, st>>>(samples, s0, buf3);
+    }
+    return cudaGetLastError();
+}
+template cudaError_t launch_fill_ghosts<double>(const SampleParams *, int, int, double *, double *, cudaStream_t);
+template cudaError_t launch_fill_ghosts<float>(const SampleParams *, int, int, float *, float *, cudaStream_t);
 
 // per-sample residual = sqrt(sum / (Nx Ny)) (runOne, cpuLBM.cpp:2322-2331)
 __global__ void k_residual(const SampleParams *samples, int nsamples, const double *partial, const int *tile_first,

@@ -87,6 +87,10 @@ template <class S>
 cudaError_t launch_set_macro(const SampleParams *samples, int s, S *state, S *buf2, S *buf3, const double *fields,
                              const uint8_t *nflags, const double *fref, long long nodes, cudaStream_t st);
 cudaError_t launch_wait_selftest(int *status, int arrive, cudaStream_t st);
+// copy the edge columns of stage buffers 2 and 3 into the ghost columns
+// (SampleParams::gx) of samples s0 .. s0 + ns - 1 (after their state was set)
+template <class S>
+cudaError_t launch_fill_ghosts(const SampleParams *samples, int s0, int ns, S *buf2, S *buf3, cudaStream_t st);
 cudaError_t launch_residual(const SampleParams *samples, int nsamples, const double *partial, const int *tile_first,
                             const int *tile_count, double *residual, cudaStream_t st);
 

@@ -283,8 +283,9 @@ struct lbm_server {
         r->nx = h.nx;
         r->ny = h.ny;
         r->steps_total = h.nsteps;
-        r->nodes = r->ps.p.plane;
-        cut_tiles(r->ps.flags.data(), r->ps.p.pitch, h.nx, h.ny, tx, ty, r->ps.p.flags, 0, r->tiles);
+        // node slots: the planes, and room for GHOST_SLACK state elements
+        r->nodes = r->ps.p.plane + (r->ps.p.gx ? (GHOST_SLACK + NPL - 1) / NPL : 0);
+        cut_tiles(r->ps.flags.data(), r->ps.p.pitch, h.nx, h.ny, tx, ty, r->ps.p.flags, r->ps.p.gx, 0, r->tiles);
         const long long n = (long long)h.nx * h.ny;
         r->fields.resize(4 * n);
         for (int x = 0; x < h.nx; ++x)
@@ -375,7 +376,8 @@ struct lbm_server {
             Request *r = packed[k];
             SampleParams p = r->ps.p;
             p.node_off = r->node_off;
-            p.state_off = (long long)NPL * r->node_off;
+            // the first row's left ghosts (SampleParams::gx) before plane 0
+            p.state_off = (long long)NPL * r->node_off + (p.gx ? GHOST_SLACK : 0);
             p.xoff = (int)v_tdx.size();
             p.yoff = (int)v_tdy.size();
             p.first_tile = (int)tiles_all.size();
@@ -435,6 +437,9 @@ struct lbm_server {
         }
         split_runs(d_tiles_rk3.p, (int)tiles_rk3.size(), ns_rk3, nw_rk3, lists.rk3_simple, lists.rk3_wrap,
                    lists.rk3_general);
+        lists.samples = d_sp.p;
+        lists.nsamples = (int)sp.size();
+        lists.any_ghost = std::any_of(sp.begin(), sp.end(), [](const SampleParams &q) { return q.gx != 0; });
         lists.walls_all = d_walls_all.p;
         lists.n_walls_all = (int)walls_all.size();
         lists.walls_rk3 = d_walls_rk3.p;
@@ -612,6 +617,15 @@ struct lbm_server {
         else
             CU(launch_set_macro<float>(d_sp.p, k, reinterpret_cast<float *>(state.p), reinterpret_cast<float *>(buf2.p),
                                        reinterpret_cast<float *>(buf3.p), scratch.p, nflags.p, d_fref.p, n, stream));
+        // the ghost columns of the new solve's stage buffers (SampleParams::gx)
+        if (r->ps.p.gx) {
+            if (prec == LBM_PREC_F64)
+                CU(launch_fill_ghosts<double>(d_sp.p, k, 1, reinterpret_cast<double *>(buf2.p),
+                                              reinterpret_cast<double *>(buf3.p), stream));
+            else
+                CU(launch_fill_ghosts<float>(d_sp.p, k, 1, reinterpret_cast<float *>(buf2.p),
+                                             reinterpret_cast<float *>(buf3.p), stream));
+        }
     }
 
     double *result_ptr(const Request *r) const
