@@ -93,7 +93,67 @@ __constant__ int c_MIR_EW[NQ] = {0, 3, 2, 1, 4, 6, 5, 8, 7, 11, 10, 9, 12};
 constexpr int kEX[NQ] = {0, 1, 0, -1, 0, 1, -1, -1, 1, 2, 0, -2, 0};
 constexpr int kEY[NQ] = {0, 0, 1, 0, -1, 1, 1, -1, -1, 0, 2, 0, -2};
 
+// the same as functions: compile-time values in unrolled loops, no table
+__host__ __device__ constexpr int lat_ex(int i)
+{
+    return (i == 1 || i == 5 || i == 8) ? 1 : (i == 3 || i == 6 || i == 7) ? -1 : i == 9 ? 2 : i == 11 ? -2 : 0;
+}
+__host__ __device__ constexpr int lat_ey(int i)
+{
+    return (i == 2 || i == 5 || i == 6) ? 1 : (i == 4 || i == 7 || i == 8) ? -1 : i == 10 ? 2 : i == 12 ? -2 : 0;
+}
+constexpr bool lat_fn_match()
+{
+    for (int i = 0; i < NQ; ++i)
+        if (lat_ex(i) != kEX[i] || lat_ey(i) != kEY[i]) return false;
+    return true;
+}
+static_assert(lat_fn_match(), "lattice functions differ from the table");
+
 __device__ __forceinline__ int isgn(int a) { return (a > 0) - (a < 0); }
+
+// Round-to-nearest operations the compiler may neither fuse nor split:
+// NND, WENO5 and the FP32 equilibria are written with them so that every
+// compiled instance (the simple-tile paths per scheme, the boundary-aware
+// paths, the wall factors, the tile-shape instances) rounds a node the same
+// way, and results do not depend on which path a node took (tile shape,
+// batch packing).
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float xneg(float a) { return -a; }
+__device__ __forceinline__ double xneg(double a) { return -a; }
+__device__ __forceinline__ float xmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double xmin(double a, double b) { return fmin(a, b); }
+// The same operations on a packed pair of FP32 values (the f and h planes
+// of one face), one sm_100 f32x2 instruction each: every lane is rounded
+// exactly as the scalar operation rounds it, so a face reconstructed in
+// pairs equals the scalar reconstruction bit for bit.  a - b is formed as
+// fma(b, -1, a), which is a - b correctly rounded.
+__device__ __forceinline__ float2 xmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 xadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 xsub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 xfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 xneg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 xmin(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+
+// a constant in the arithmetic type (both lanes of a pair)
+template <class C>
+__device__ __forceinline__ C kc(double v) { return C(v); }
+template <>
+__device__ __forceinline__ float2 kc<float2>(double v) { return make_float2((float)v, (float)v); }
+// FP32 arithmetic, scalar or packed
+template <class C>
+struct IsF32 { static constexpr bool value = false; };
+template <>
+struct IsF32<float> { static constexpr bool value = true; };
+template <>
+struct IsF32<float2> { static constexpr bool value = true; };
 
 // ------------------------------------------------------------ equilibria
 // equilibrium2D (cpuLBM.cpp:785-844) with the polynomials of
@@ -339,6 +399,143 @@ __device__ __forceinline__ void eqd_fam9(const EqDev<C> &q, C *f, C *h)
     }
 }
 
+// ------------------------- FP32 deviations: explicitly rounded, lanes paired
+// The FP32 path evaluates the deviation polynomials above with every
+// operation explicitly rounded (no compiler contraction), so every kernel
+// that computes a node's equilibria gives it the same bits.  The terms are
+// those of the generic form, regrouped (common factors, Horner form).  In
+// families 1 and 9 the two axis pairs (k = 0: U = u, W = v; k = 1: U = v,
+// W = u) are the two lanes of packed f32x2 operations; in family 5 the
+// lanes are the sign of u in f (for v + and -) and (OE, EO) in h.
+__device__ __forceinline__ float2 bc2(float s) { return make_float2(s, s); }
+
+__device__ __forceinline__ void eqd_fam0(const EqDev<float> &q, float &f0, float &h0)
+{
+    const float u = q.u, v = q.v, T = q.T, K = q.K, T0 = q.T0, tau = q.tau;
+    const float a = xmul(u, u), c = xmul(v, v), s2 = xadd(a, c), pc = xmul(a, c), T2 = xmul(T, T);
+    const float S2 = xadd(T, T0), S3 = xfma(T, S2, xmul(T0, T0));
+    // dP = s2 (5/2 T - 5/4 + s2/4) + pc/2 + 5/2 tau (S2 - 1), P0 = 1 + 5/2 T0 (T0 - 1)
+    const float dP = xfma(s2, xfma(0.25f, s2, xfma(2.5f, T, -1.25f)),
+                          xfma(0.5f, pc, xmul(xmul(2.5f, tau), xadd(S2, -1.0f))));
+    const float P0 = xfma(xmul(2.5f, T0), xadd(T0, -1.0f), 1.0f);
+    f0 = xfma(q.rho, dP, xmul(q.drho, P0));
+    // dQ = T2 (5/4 K + 45/4) s2 + T (s2 ((K/8 + 5/2) s2 - 5/8 K - 5) + (K/4 + 5/2) pc)
+    //      + s2 (s2 (s2/8 - 5/8) + pc/4 + 1/2) + tau (k3 S3 + k2 S2 + k1),
+    // Q0 = T0 (T0 (T0 k3 + k2) + k1)
+    const float k3 = xfma(1.25f, K, 20.0f / 3.0f), k2 = xfma(-1.25f, K, -5.0f), k1 = xfma(0.5f, K, 1.0f);
+    const float tT = xfma(s2, xfma(xfma(0.125f, K, 2.5f), s2, xfma(-0.625f, K, -5.0f)), xmul(xfma(0.25f, K, 2.5f), pc));
+    const float rest = xmul(s2, xfma(s2, xfma(0.125f, s2, -0.625f), xfma(0.25f, pc, 0.5f)));
+    const float tG = xmul(tau, xfma(k3, S3, xfma(k2, S2, k1)));
+    const float dQ = xfma(T2, xmul(xfma(1.25f, K, 11.25f), s2), xfma(T, tT, xadd(rest, tG)));
+    const float Q0 = xmul(T0, xfma(T0, xfma(T0, k3, k2), k1));
+    h0 = xmul(q.RTc, xfma(q.rho, dQ, xmul(q.drho, Q0)));
+}
+
+__device__ __forceinline__ void eqd_fam1(const EqDev<float> &q, float *f, float *h)
+{
+    const float T = q.T, K = q.K, T0 = q.T0, tau = q.tau, T2 = xmul(T, T);
+    const float S2 = xadd(T, T0), S3 = xfma(T, S2, xmul(T0, T0));
+    const float kh3 = xfma(-0.5f, K, -8.0f / 3.0f), kh2 = xfma(K, 1.0f / 3.0f, 4.0f / 3.0f);
+    const float P0 = xmul(T0, xsub(2.0f / 3.0f, T0));
+    const float Q0 = xmul(xmul(T0, T0), xfma(T0, kh3, kh2));
+    const float tGf = xmul(tau, xsub(2.0f / 3.0f, S2));
+    const float tGh = xmul(tau, xfma(kh3, S3, xmul(kh2, S2)));
+    const float2 U = make_float2(q.u, q.v), W = make_float2(q.v, q.u);
+    const float2 A = xmul(U, U), Cc = xmul(W, W), vT = bc2(T), vT2 = bc2(T2), vr = bc2(q.rho);
+    // f: E = T (-3/2 A - Cc/2) + A (m - A/6) + tau Gf, O = U (m - T - A/6), m = 2/3 - Cc/2
+    const float2 m = xfma(kc<float2>(-0.5), Cc, kc<float2>(2.0 / 3.0));
+    const float2 Ef = xfma(vT, xfma(kc<float2>(-1.5), A, xmul(kc<float2>(-0.5), Cc)),
+                           xfma(A, xfma(kc<float2>(-1.0 / 6.0), A, m), bc2(tGf)));
+    const float2 Of = xmul(U, xfma(kc<float2>(-1.0 / 6.0), A, xsub(m, vT)));
+    const float2 dP0 = bc2(xmul(q.drho, P0));
+    const float2 fp = xfma(vr, xadd(Ef, Of), dP0), fm = xfma(vr, xsub(Ef, Of), dP0);
+    f[0] = fp.x; f[1] = fp.y; f[2] = fm.x; f[3] = fm.y;
+    // h: with CB = Cc (1/3 - Cc/4) and R = A (1/3 - A/12 - Cc/3) + CB,
+    // E = T2 (c1 A + c2 Cc) + T (A (c3 A + c4 Cc + c5) + CB) + A R + tau Gh,
+    // O = U (T2 c8 + T (c6 A + c2 Cc + kh2) + R)
+    const float c1 = xfma(-0.75f, K, -6.5f), c2 = xfma(-0.25f, K, -2.5f), c3 = xfma(K, -1.0f / 12.0f, -19.0f / 12.0f);
+    const float c4 = xfma(-0.25f, K, -3.5f), c5 = xfma(K, 1.0f / 3.0f, 7.0f / 3.0f), c6 = xfma(K, -1.0f / 12.0f, -7.0f / 6.0f);
+    const float c8 = xfma(-0.5f, K, -3.0f);
+    const float2 CB = xmul(Cc, xfma(kc<float2>(-0.25), Cc, kc<float2>(1.0 / 3.0)));
+    const float2 R = xfma(A, xfma(kc<float2>(-1.0 / 12.0), A, xfma(kc<float2>(-1.0 / 3.0), Cc, kc<float2>(1.0 / 3.0))), CB);
+    const float2 Eh = xfma(vT2, xfma(bc2(c1), A, xmul(bc2(c2), Cc)),
+                           xfma(vT, xfma(A, xfma(bc2(c3), A, xfma(bc2(c4), Cc, bc2(c5))), CB), xfma(A, R, bc2(tGh))));
+    const float2 Oh = xmul(U, xfma(vT2, bc2(c8), xfma(vT, xfma(bc2(c6), A, xfma(bc2(c2), Cc, bc2(kh2))), R)));
+    const float2 dQ0 = bc2(xmul(q.drho, Q0)), vR = bc2(q.RTc);
+    const float2 hp = xmul(vR, xfma(vr, xadd(Eh, Oh), dQ0)), hm = xmul(vR, xfma(vr, xsub(Eh, Oh), dQ0));
+    h[0] = hp.x; h[1] = hp.y; h[2] = hm.x; h[3] = hm.y;
+}
+
+__device__ __forceinline__ void eqd_fam5(const EqDev<float> &q, float *f, float *h)
+{
+    const float u = q.u, v = q.v, T = q.T, K = q.K, T0 = q.T0, tau = q.tau;
+    const float a = xmul(u, u), c = xmul(v, v), s2 = xadd(a, c), pc = xmul(a, c), T2 = xmul(T, T);
+    const float S2 = xadd(T, T0), S3 = xfma(T, S2, xmul(T0, T0));
+    // f = rho (base + (T (X + Y) + X Y)/4) + drho P0, X = a +- u, Y = c +- v
+    const float P0 = xmul(0.25f, xmul(T0, T0)), base = xmul(xmul(0.25f, tau), S2);
+    const float2 X = make_float2(xadd(a, u), xsub(a, u));
+    const float2 vT = bc2(T), vr = bc2(q.rho), vb = bc2(base), dP0 = bc2(xmul(q.drho, P0));
+    const float2 Yp = bc2(xadd(c, v)), Ym = bc2(xsub(c, v));
+    const float2 fp = xfma(vr, xfma(kc<float2>(0.25), xfma(X, Yp, xmul(vT, xadd(X, Yp))), vb), dP0);
+    const float2 fm = xfma(vr, xfma(kc<float2>(0.25), xfma(X, Ym, xmul(vT, xadd(X, Ym))), vb), dP0);
+    f[0] = fp.x; f[1] = fp.y; f[2] = fm.y; f[3] = fm.x;
+    // h = RTc (rho (EE +- OE +- EO +- OO) + drho Q0) with
+    // EE = T2 (k8 + 9/8) s2 + T ((k8 + 5/4) pc + s2^2/8) + pc s2/8 + tau (k8 + 2/3) S3,
+    // (OE, EO) = (u, v) (T2 (k8 + 3/4) + T ((k8 + 9/8) (c, a) + (a, c)/8) + (c, a) s2/8),
+    // OO = u v (T (k8 + 3/4) + s2/8)
+    const float k8 = xmul(0.125f, K), e1 = xadd(k8, 0.75f), e2 = xadd(k8, 1.125f), e3 = xadd(k8, 2.0f / 3.0f);
+    const float Q0 = xmul(xmul(xmul(T0, T0), T0), e3);
+    const float EE = xfma(T2, xmul(e2, s2),
+                          xfma(T, xfma(xadd(k8, 1.25f), pc, xmul(0.125f, xmul(s2, s2))),
+                               xfma(xmul(0.125f, pc), s2, xmul(xmul(tau, e3), S3))));
+    const float2 P = make_float2(a, c), Q = make_float2(c, a);
+    const float2 OEO = xmul(make_float2(u, v),
+                            xfma(bc2(T2), bc2(e1), xfma(vT, xfma(bc2(e2), Q, xmul(kc<float2>(0.125), P)),
+                                                         xmul(kc<float2>(0.125), xmul(Q, bc2(s2))))));
+    const float OO = xmul(xmul(u, v), xfma(T, e1, xmul(0.125f, s2)));
+    const float p = xadd(EE, OO), mm = xsub(EE, OO), so = xadd(OEO.x, OEO.y), dd = xsub(OEO.x, OEO.y);
+    const float2 vR = bc2(q.RTc), dQ0 = bc2(xmul(q.drho, Q0));
+    const float2 h01 = xmul(vR, xfma(vr, make_float2(xadd(p, so), xsub(mm, dd)), dQ0));
+    const float2 h23 = xmul(vR, xfma(vr, make_float2(xsub(p, so), xadd(mm, dd)), dQ0));
+    h[0] = h01.x; h[1] = h01.y; h[2] = h23.x; h[3] = h23.y;
+}
+
+__device__ __forceinline__ void eqd_fam9(const EqDev<float> &q, float *f, float *h)
+{
+    const float T = q.T, K = q.K, T0 = q.T0, tau = q.tau, T2 = xmul(T, T);
+    const float S2 = xadd(T, T0), S3 = xfma(T, S2, xmul(T0, T0));
+    const float kh3 = xfma(K, 1.0f / 16.0f, 1.0f / 3.0f), kh2 = xfma(K, -1.0f / 48.0f, -1.0f / 12.0f);
+    const float P0 = xmul(T0, xfma(0.125f, T0, -1.0f / 24.0f));
+    const float Q0 = xmul(xmul(T0, T0), xfma(T0, kh3, kh2));
+    const float tGf = xmul(tau, xfma(0.125f, S2, -1.0f / 24.0f));
+    const float tGh = xmul(tau, xfma(kh3, S3, xmul(kh2, S2)));
+    const float2 U = make_float2(q.u, q.v), W = make_float2(q.v, q.u);
+    const float2 A = xmul(U, U), Cc = xmul(W, W), vT = bc2(T), vT2 = bc2(T2), vr = bc2(q.rho);
+    const float2 qT = bc2(xmul(0.25f, T)), Am1 = xadd(A, kc<float2>(-1.0));
+    // f: E = A (T/4 + (A - 1)/24) + tau Gf, O = U (T/4 + (A - 1)/12)
+    const float2 Ef = xfma(A, xfma(kc<float2>(1.0 / 24.0), Am1, qT), bc2(tGf));
+    const float2 Of = xmul(U, xfma(kc<float2>(1.0 / 12.0), Am1, qT));
+    const float2 dP0 = bc2(xmul(q.drho, P0));
+    const float2 fp = xfma(vr, xadd(Ef, Of), dP0), fm = xfma(vr, xsub(Ef, Of), dP0);
+    f[0] = fp.x; f[1] = fp.y; f[2] = fm.x; f[3] = fm.y;
+    // h: with M = (A + Cc)(A - 1),
+    // E = T2 (d1 A + Cc/16) + T (A (d2 A + Cc/8 - d3) - Cc/48) + A M/48 + tau Gh,
+    // O = U (T2 d4 + T (d5 A + Cc/8 + d6) + M/24)
+    const float d1 = xfma(0.125f, K, 17.0f / 16.0f), d2 = xfma(K, 1.0f / 48.0f, 1.0f / 3.0f);
+    const float d3 = xfma(K, 1.0f / 48.0f, 7.0f / 48.0f), d4 = xfma(0.125f, K, 0.75f);
+    const float d5 = xfma(K, 1.0f / 24.0f, 11.0f / 24.0f), d6 = xfma(K, -1.0f / 24.0f, -1.0f / 6.0f);
+    const float2 M = xmul(xadd(A, Cc), Am1);
+    const float2 Eh = xfma(vT2, xfma(bc2(d1), A, xmul(kc<float2>(1.0 / 16.0), Cc)),
+                           xfma(vT, xfma(A, xfma(bc2(d2), A, xfma(kc<float2>(0.125), Cc, bc2(xneg(d3)))),
+                                         xmul(kc<float2>(-1.0 / 48.0), Cc)),
+                                xfma(kc<float2>(1.0 / 48.0), xmul(A, M), bc2(tGh))));
+    const float2 Oh = xmul(U, xfma(vT2, bc2(d4), xfma(vT, xfma(bc2(d5), A, xfma(kc<float2>(0.125), Cc, bc2(d6))),
+                                                      xmul(kc<float2>(1.0 / 24.0), M))));
+    const float2 dQ0 = bc2(xmul(q.drho, Q0)), vR = bc2(q.RTc);
+    const float2 hp = xmul(vR, xfma(vr, xadd(Eh, Oh), dQ0)), hm = xmul(vR, xfma(vr, xsub(Eh, Oh), dQ0));
+    h[0] = hp.x; h[1] = hp.y; h[2] = hm.x; h[3] = hm.y;
+}
+
 // Equilibria of one family in the stored representation: full values on the
 // FP64 path, deviations from the rest state on the FP32 path.
 template <class C, bool DEV>
@@ -450,48 +647,6 @@ __device__ __forceinline__ float2 minmod<float2>(float2 a, float2 b)
     return make_float2(minmod<float>(a.x, b.x), minmod<float>(a.y, b.y));
 }
 
-// Round-to-nearest operations the compiler may neither fuse nor split:
-// NND and WENO5 are written with them so that every compiled instance (the
-// simple-tile paths per scheme, the boundary-aware paths, the wall factors)
-// rounds a face flux the same way, and results do not depend on which path
-// a node took (tile shape, batch packing).
-__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
-__device__ __forceinline__ float xneg(float a) { return -a; }
-__device__ __forceinline__ double xneg(double a) { return -a; }
-__device__ __forceinline__ float xmin(float a, float b) { return fminf(a, b); }
-__device__ __forceinline__ double xmin(double a, double b) { return fmin(a, b); }
-// The same operations on a packed pair of FP32 values (the f and h planes
-// of one face), one sm_100 f32x2 instruction each: every lane is rounded
-// exactly as the scalar operation rounds it, so a face reconstructed in
-// pairs equals the scalar reconstruction bit for bit.  a - b is formed as
-// fma(b, -1, a), which is a - b correctly rounded.
-__device__ __forceinline__ float2 xmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 xadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 xsub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
-__device__ __forceinline__ float2 xfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 xneg(float2 a) { return make_float2(-a.x, -a.y); }
-__device__ __forceinline__ float2 xmin(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
-
-// a constant in the arithmetic type (both lanes of a pair)
-template <class C>
-__device__ __forceinline__ C kc(double v) { return C(v); }
-template <>
-__device__ __forceinline__ float2 kc<float2>(double v) { return make_float2((float)v, (float)v); }
-// FP32 arithmetic, scalar or packed
-template <class C>
-struct IsF32 { static constexpr bool value = false; };
-template <>
-struct IsF32<float> { static constexpr bool value = true; };
-template <>
-struct IsF32<float2> { static constexpr bool value = true; };
-
 // NND (cpuLBM.cpp:1328-1356) on the 3 upwind-ordered values s0, s1, s2
 template <class C>
 __device__ __forceinline__ C nnd3(C ae, C s0, C s1, C s2)
@@ -502,10 +657,21 @@ __device__ __forceinline__ C nnd3(C ae, C s0, C s1, C s2)
 
 // one division per face (the FP64 path keeps it correctly rounded)
 __device__ __forceinline__ double face_div(double n, double d) { return n / d; }
-__device__ __forceinline__ float face_div(float n, float d) { return __fdividef(n, d); }
+// FP32: n times the approximate reciprocal of d (PTX rcp.approx, then one
+// correctly rounded product).  Inline PTX, so that no compiled instance may
+// lower the division another way: a face then rounds the same in every
+// kernel that reconstructs it.  d here is a positive normal number (a sum
+// of weights, or eps + b_k).
+__device__ __forceinline__ float rcp_approx(float d)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+    return r;
+}
+__device__ __forceinline__ float face_div(float n, float d) { return __fmul_rn(n, rcp_approx(d)); }
 __device__ __forceinline__ float2 face_div(float2 n, float2 d)
 {
-    return make_float2(__fdividef(n.x, d.x), __fdividef(n.y, d.y));
+    return __fmul2_rn(n, make_float2(rcp_approx(d.x), rcp_approx(d.y)));
 }
 
 // WENO5 (cpuLBM.cpp:1358-1403): Jiang-Shu indicators b_k, linear weights

@@ -90,19 +90,41 @@ __global__ void k_init(KArgs<S> a, const double *__restrict__ rho, const double 
 // ------------------------------------------------------------------ moments
 // macroPropShort of one node from its 26 stored values, read through
 // rd(p) (p = i for f_i, NQ + i for h_i).
+// The momentum sums are formed as sums of the values times the directions'
+// integer components (0, +-1, +-2: exact, and no operation for 0 in the
+// unrolled loops), scaled by c once.
+__device__ __forceinline__ void mom_add(double &acc, int e, double v)
+{
+    if (e == 1) acc += v;
+    else if (e == -1) acc -= v;
+    else if (e != 0) acc = fma((double)e, v, acc);
+}
+
+// e_i . (cu, cv) for direction i, with cu = c u and cv = c v: the
+// components are 0, +-1 or +-2, so each term is exact and only a diagonal
+// direction adds (i a compile-time value in the unrolled loops)
+template <class C>
+__device__ __forceinline__ C e_dot(int i, C cu, C cv)
+{
+    const int ex = lat_ex(i), ey = lat_ey(i);
+    const C x = ex == 1 ? cu : ex == -1 ? -cu : C(ex) * cu;
+    const C y = ey == 1 ? cv : ey == -1 ? -cv : C(ey) * cv;
+    return ex == 0 ? y : ey == 0 ? x : xadd(x, y);
+}
+
 template <class RD>
 __device__ __forceinline__ Macro node_macro_rd(RD rd, const SampleParams &sp)
 {
-    double r = 0, rux = 0, ruy = 0, sh = 0;
+    double r = 0, rx = 0, ry = 0, sh = 0;
 #pragma unroll
     for (int i = 0; i < NQ; ++i) {
         const double fv = (double)rd(i);
         r += fv;
-        rux += fv * (sp.c * c_EX[i]);
-        ruy += fv * (sp.c * c_EY[i]);
+        mom_add(rx, lat_ex(i), fv);
+        mom_add(ry, lat_ey(i), fv);
         sh += (double)rd(NQ + i);
     }
-    return macro_from_sums(r, rux, ruy, sh, sp);
+    return macro_from_sums(r, sp.c * rx, sp.c * ry, sh, sp);
 }
 
 // the same with stn the node's element in plane 0, the planes sp.plane
@@ -120,16 +142,16 @@ __device__ __forceinline__ Macro node_macro(const S *__restrict__ stn, const Sam
 template <class S>
 __device__ __forceinline__ Macro node_macro_at(const S *__restrict__ st, const SampleParams &sp, long long o)
 {
-    double r = 0, rux = 0, ruy = 0, sh = 0;
+    double r = 0, rx = 0, ry = 0, sh = 0;
 #pragma unroll
     for (int i = 0; i < NQ; ++i) {
         const double fv = (double)st[(long long)i * sp.plane + o];
         r += fv;
-        rux += fv * (sp.c * c_EX[i]);
-        ruy += fv * (sp.c * c_EY[i]);
+        mom_add(rx, lat_ex(i), fv);
+        mom_add(ry, lat_ey(i), fv);
         sh += (double)st[(long long)(NQ + i) * sp.plane + o];
     }
-    return macro_from_sums(r, rux, ruy, sh, sp);
+    return macro_from_sums(r, sp.c * rx, sp.c * ry, sh, sp);
 }
 
 // ------------------------------------------------------------------- P0
@@ -176,7 +198,7 @@ __global__ void __launch_bounds__(256, Stage0Blocks<S>::value) k_stage0(KArgs<S>
         if (fabs(sf - (m.rho - sp.rho0)) > a.eq_tol * (sizeof(C) == 8 ? 1.0 : fmax(1.0, fabs(m.rho))))
             atomicOr(&a.status[t.sample], STATUS_EQ);
     }
-    const C dt = (C)sp.dt, ux = (C)m.ux, uy = (C)m.uy;
+    const C dt = (C)sp.dt, cu = (C)sp.c * (C)m.ux, cv = (C)sp.c * (C)m.uy;
     const C rq = (C)m.q, Pr = (C)sp.Pr;  // 1/tau_f
     if (RK == 1) {
         // RK3 stages 1 and 2 (cpuLBM.cpp:1819-1924); stage 2 reuses stage 1's
@@ -188,7 +210,7 @@ __global__ void __launch_bounds__(256, Stage0Blocks<S>::value) k_stage0(KArgs<S>
 #pragma unroll
         for (int i = 0; i < NQ; ++i) {
             const C f = (C)st[(long long)i * sp.plane + o], h = (C)st[(long long)(NQ + i) * sp.plane + o];
-            const C eu = (C)(sp.c * c_EX[i]) * ux + (C)(sp.c * c_EY[i]) * uy;
+            const C eu = e_dot<C>(i, cu, cv);
             const C f1 = (f + cf * fe[i]) * icf;
             const C h1 = (h - hdt * g * eu * (fe[i] - f1) + ch * he[i]) * ich;
             const C f2 = (f - cf * (fe[i] - f1) + cf * fe[i]) * icf;
@@ -203,7 +225,7 @@ __global__ void __launch_bounds__(256, Stage0Blocks<S>::value) k_stage0(KArgs<S>
 #pragma unroll
         for (int i = 0; i < NQ; ++i) {
             const C f = (C)st[(long long)i * sp.plane + o], h = (C)st[(long long)(NQ + i) * sp.plane + o];
-            const C eu = (C)(sp.c * c_EX[i]) * ux + (C)(sp.c * c_EY[i]) * uy;
+            const C eu = e_dot<C>(i, cu, cv);
             const C f1 = (f + cf * fe[i]) * icf;
             const C h1 = (h - dt * eu * ((fe[i] - f1) * g) + ch * he[i]) * ich;
             b2[(long long)i * sp.plane + o] = (S)f1;
@@ -1019,27 +1041,31 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             C rq1, rq3, ux1, uy1, ux3, uy3;
             double rho3;
             {
-                m1 = node_macro_rd(rd, sp);
-                rq1 = (C)m1.q; ux1 = (C)m1.ux; uy1 = (C)m1.uy;
-            }
-            {
-                double r = 0, rux = 0, ruy = 0, sh = 0;
+                // one pass over the values for both
+                double r1 = 0, x1 = 0, y1 = 0, s1 = 0, r3 = 0, x3 = 0, y3 = 0, s3 = 0;
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) {
-                    const double fv = (double)rd(i);
-                    const double Df = (double)sD[i * NT + tid];
-                    r += fv - Df;
-                    rux += fv * (sp.c * c_EX[i]) - Df * (sp.c * c_EX[i]);
-                    ruy += fv * (sp.c * c_EY[i]) - Df * (sp.c * c_EY[i]);
-                    sh += (double)rd(NQ + i) - (double)sD[(NQ + i) * NT + tid];
+                    const double fv = (double)rd(i), hv = (double)rd(NQ + i);
+                    const double d = fv - (double)sD[i * NT + tid];
+                    r1 += fv;
+                    mom_add(x1, lat_ex(i), fv);
+                    mom_add(y1, lat_ey(i), fv);
+                    s1 += hv;
+                    r3 += d;
+                    mom_add(x3, lat_ex(i), d);
+                    mom_add(y3, lat_ey(i), d);
+                    s3 += hv - (double)sD[(NQ + i) * NT + tid];
                 }
-                m3 = macro_from_sums(r, rux, ruy, sh, sp);
+                m1 = macro_from_sums(r1, sp.c * x1, sp.c * y1, s1, sp);
+                m3 = macro_from_sums(r3, sp.c * x3, sp.c * y3, s3, sp);
+                rq1 = (C)m1.q; ux1 = (C)m1.ux; uy1 = (C)m1.uy;
                 rq3 = (C)m3.q; ux3 = (C)m3.ux; uy3 = (C)m3.uy;
                 rho3 = m3.rho;
             }
             const EqArgs<C, DEV> q1(m1.rho, m1.ux, m1.uy, m1.T, sp);
             const EqArgs<C, DEV> q3(m3.rho, m3.ux, m3.uy, m3.T, sp);
             const C hdt = dt * C(0.5);
+            const C cu1 = (C)sp.c * ux1, cv1 = (C)sp.c * uy1, cu3 = (C)sp.c * ux3, cv3 = (C)sp.c * uy3;
             // dt/(2 tau) and 1/tau of stages 2 (= 1) and 3, all from q = p/mu
             const C Pr = (C)sp.Pr;
             const C itf2 = rq1, itf3 = rq3, ith2 = Pr * rq1, ith3 = Pr * rq3;
@@ -1067,8 +1093,15 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     const int of = i * PL, oh = (NQ + i) * PL;
                     const C f = vf[k], h = vh[k], f2 = vf2[k], h2 = vh2[k];
                     const C Df = sD[i * NT + tid], Dh = sD[(NQ + i) * NT + tid];
-                    const C exi = (C)(sp.c * c_EX[i]), eyi = (C)(sp.c * c_EY[i]);
-                    const C eu2 = exi * ux1 + eyi * uy1, eu3 = exi * ux3 + eyi * uy3;
+                    C eu2, eu3;
+                    if constexpr (sizeof(S) == 4) {
+                        eu2 = e_dot<C>(i, cu1, cv1);
+                        eu3 = e_dot<C>(i, cu3, cv3);
+                    } else {
+                        const C exi = (C)(sp.c * c_EX[i]), eyi = (C)(sp.c * c_EY[i]);
+                        eu2 = exi * ux1 + eyi * uy1;
+                        eu3 = exi * ux3 + eyi * uy3;
+                    }
                     // stage 3 (cpuLBM.cpp:1970, 1986)
                     const C f3 = (f - Df + a2 * (e1f[k] - f2) + a3 * e3f[k]) * ia3;
                     const C cpl = eu2 * g2 * (e1f[k] - f2) + eu3 * g3 * (e3f[k] - f3);
@@ -1121,6 +1154,7 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             constexpr bool DEV = sizeof(S) == 4;
             const EqArgs<C, DEV> q(m.rho, m.ux, m.uy, m.T, sp);
             const C ux = (C)m.ux, uy = (C)m.uy, Pr = (C)sp.Pr;
+            const C cu = (C)sp.c * ux, cv = (C)sp.c * uy;
             const C rtf = dt * (C)m.q, rth = dt * Pr * (C)m.q, rg = (Pr - C(1)) * (C)m.q;  // dt/tau_f, dt/tau_h, 1/tau_hf
             double sf = 0;
             auto family = [&](const int fam) {
@@ -1143,7 +1177,9 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                     const int of = i * PL, oh = (NQ + i) * PL;
                     const C f = vf[k], h = vh[k];
                     const C Df = sD[i * NT + tid], Dh = sD[(NQ + i) * NT + tid];
-                    const C eu = (C)(sp.c * c_EX[i]) * ux + (C)(sp.c * c_EY[i]) * uy;
+                    C eu;
+                    if constexpr (sizeof(S) == 4) eu = e_dot<C>(i, cu, cv);
+                    else eu = (C)(sp.c * c_EX[i]) * ux + (C)(sp.c * c_EY[i]) * uy;
                     C fn, hn;
                     if (MODE == 3) {
                         const C f1 = v1f[k], h1 = v1h[k];
