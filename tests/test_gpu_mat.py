@@ -47,9 +47,10 @@ def test_fp32_from_mat_within_tolerance(cuda_device, mat_input):
     stream next to fluid at rest), so after two steps the FP32 error sits at
     the region edges, where WENO5's weights amplify rounding: moving the
     three densities by one FP32 ulp changes the relative L2 error of T by up
-    to a factor 2 (measured: 5.2e-6 on perturbed inputs, 1.0e-5 on the file's
-    own values).  The tolerance (1e-5) therefore holds for the median over
-    the file's input and four perturbed copies, each run within twice it."""
+    to a factor 4 (measured: 1.5e-6 to 2.6e-6 on perturbed inputs, 6.7e-6
+    on the file's own values).  The tolerance (1e-5) is therefore checked
+    on the median over the file's input and four perturbed copies, and each
+    run must stay within twice it."""
     p, case, ref = mat_input
     s = Solver.from_mat(p, "f32")
     s.step(int(ref["step"]))

@@ -206,15 +206,27 @@ __global__ void __launch_bounds__(256, Stage0Blocks<S>::value) k_stage0(KArgs<S>
         // ch = dt/(2 tau_h), g = 1/tau_hf.
         const C hdt = C(0.5) * dt;
         const C cf = hdt * rq, ch = hdt * Pr * rq, g = (Pr - C(1)) * rq;
-        const C icf = C(1) / (C(1) + cf), ich = C(1) / (C(1) + ch);
+        const C icf = C(1) / (C(1) + cf), ich = C(1) / (C(1) + ch), hg = hdt * g;
 #pragma unroll
         for (int i = 0; i < NQ; ++i) {
             const C f = (C)st[(long long)i * sp.plane + o], h = (C)st[(long long)(NQ + i) * sp.plane + o];
             const C eu = e_dot<C>(i, cu, cv);
-            const C f1 = (f + cf * fe[i]) * icf;
-            const C h1 = (h - hdt * g * eu * (fe[i] - f1) + ch * he[i]) * ich;
-            const C f2 = (f - cf * (fe[i] - f1) + cf * fe[i]) * icf;
-            const C h2 = (h - hdt * (eu * g * (fe[i] - f2) - eu * g * (fe[i] - f1)) - ch * (he[i] - h1) + ch * he[i]) * ich;
+            C f2, h2;
+            if constexpr (sizeof(S) == 4) {
+                // FP32, explicitly rounded, with the stage-2 forms reduced:
+                // -cf (fe - f1) + cf fe = cf f1, -ch (he - h1) + ch he = ch h1,
+                // and the two coupling terms combine to hdt g eu (f1 - f2)
+                const C hge = xmul(hg, eu);
+                const C f1 = xmul(xfma(cf, fe[i], f), icf);
+                const C h1 = xmul(xsub(xfma(ch, he[i], h), xmul(hge, xsub(fe[i], f1))), ich);
+                f2 = xmul(xfma(cf, f1, f), icf);
+                h2 = xmul(xfma(ch, h1, xsub(h, xmul(hge, xsub(f1, f2)))), ich);
+            } else {
+                const C f1 = (f + cf * fe[i]) * icf;
+                const C h1 = (h - hdt * g * eu * (fe[i] - f1) + ch * he[i]) * ich;
+                f2 = (f - cf * (fe[i] - f1) + cf * fe[i]) * icf;
+                h2 = (h - hdt * (eu * g * (fe[i] - f2) - eu * g * (fe[i] - f1)) - ch * (he[i] - h1) + ch * he[i]) * ich;
+            }
             b2[(long long)i * sp.plane + o] = (S)f2;
             b2[(long long)(NQ + i) * sp.plane + o] = (S)h2;
         }
@@ -1102,13 +1114,32 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
                         eu2 = exi * ux1 + eyi * uy1;
                         eu3 = exi * ux3 + eyi * uy3;
                     }
-                    // stage 3 (cpuLBM.cpp:1970, 1986)
-                    const C f3 = (f - Df + a2 * (e1f[k] - f2) + a3 * e3f[k]) * ia3;
-                    const C cpl = eu2 * g2 * (e1f[k] - f2) + eu3 * g3 * (e3f[k] - f3);
-                    const C h3 = (h - Dh - hdt * cpl + b2c * (e1h[k] - h2) + b3c * e3h[k]) * ib3;
-                    // update without the stage-3 fluxes (cpuLBM.cpp:2022, 2039)
-                    const C accf = f - C(0.5) * Df + hdt * ((e1f[k] - f2) * itf2 + (e3f[k] - f3) * itf3);
-                    const C acch = h - C(0.5) * Dh + hdt * ((e1h[k] - h2) * ith2 + (e3h[k] - h3) * ith3) - hdt * cpl;
+                    // stage 3 (cpuLBM.cpp:1970, 1986) and the update without
+                    // the stage-3 fluxes (cpuLBM.cpp:2022, 2039)
+                    C f3, h3, accf, acch;
+                    if constexpr (sizeof(S) == 4) {
+                        // FP32: the f and h lanes as packed pairs, every
+                        // operation explicitly rounded
+                        // (a2, b2c) = hdt (1/tau_f, 1/tau_h) of stage 2, (a3, b3c) of stage 3
+                        const float2 A2 = make_float2(a2, b2c), A3 = make_float2(a3, b3c);
+                        const float2 D = make_float2(Df, Dh), E3 = make_float2(e3f[k], e3h[k]);
+                        const float2 D1 = xsub(make_float2(e1f[k], e1h[k]), make_float2(f2, h2));
+                        const float2 V = make_float2(f, h);
+                        const float2 X = xfma(A2, D1, xfma(A3, E3, xsub(V, D)));
+                        f3 = xmul(X.x, ia3);
+                        // hdt times the coupling term cpl
+                        const float hc = xmul(hdt, xfma(xmul(eu2, g2), D1.x, xmul(xmul(eu3, g3), xsub(E3.x, f3))));
+                        h3 = xmul(xsub(X.y, hc), ib3);
+                        const float2 acc = xfma(A3, xsub(E3, make_float2(f3, h3)), xfma(A2, D1, xfma(kc<float2>(-0.5), D, V)));
+                        accf = acc.x;
+                        acch = xsub(acc.y, hc);
+                    } else {
+                        f3 = (f - Df + a2 * (e1f[k] - f2) + a3 * e3f[k]) * ia3;
+                        const C cpl = eu2 * g2 * (e1f[k] - f2) + eu3 * g3 * (e3f[k] - f3);
+                        h3 = (h - Dh - hdt * cpl + b2c * (e1h[k] - h2) + b3c * e3h[k]) * ib3;
+                        accf = f - C(0.5) * Df + hdt * ((e1f[k] - f2) * itf2 + (e3f[k] - f3) * itf3);
+                        acch = h - C(0.5) * Dh + hdt * ((e1h[k] - h2) * ith2 + (e3h[k] - h3) * ith3) - hdt * cpl;
+                    }
                     b3[of] = (S)f3;
                     b3[oh] = (S)h3;
                     if (gd) {
