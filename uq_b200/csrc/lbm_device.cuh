@@ -113,8 +113,9 @@ static_assert(lat_fn_match(), "lattice functions differ from the table");
 __device__ __forceinline__ int isgn(int a) { return (a > 0) - (a < 0); }
 
 // Round-to-nearest operations the compiler may neither fuse nor split:
-// NND, WENO5 and, on the FP32 path, the equilibria and the RK3 stage
-// updates are written with them so that every compiled instance (the
+// NND, WENO5, the flux divergence, the wall fluxes and, on the FP32 path,
+// the equilibria and the RK3 stage updates are written with them so that
+// every compiled instance (the
 // simple-tile paths per scheme, the boundary-aware
 // paths, the wall factors, the tile-shape instances) rounds a node the same
 // way, and results do not depend on which path a node took (tile shape,

@@ -412,6 +412,22 @@ __device__ __forceinline__ float2 box_flux2(const S *cf, const S *ch, int st, fl
 #undef UQ_PAIR
 }
 
+// Both planes of a face at a plain node from the staged box (f at cf, h at
+// ch): one packed pair when the scheme is fixed at compile time in FP32,
+// else two scalar reconstructions; the same values either way.
+template <class S, class C, int FM>
+__device__ __forceinline__ void box_flux_fh(const SampleParams &sp, const S *cf, const S *ch, int st, C ae, C &a, C &b)
+{
+    if constexpr (FM >= 0 && std::is_same<C, float>::value) {
+        const float2 v = box_flux2<S, FM>(cf, ch, st, ae);
+        a = v.x;
+        b = v.y;
+    } else {
+        a = box_flux<S, C, FM>(sp, cf, st, ae);
+        b = box_flux<S, C, FM>(sp, ch, st, ae);
+    }
+}
+
 // simple FP32 tiles reconstruct the f and h planes of a face as one pair
 template <class C, bool SIMPLE, int FM>
 struct PairFaces {
@@ -513,7 +529,7 @@ __device__ __forceinline__ C any_node_flux(TileCtx<S, C> &k, const S *box, int i
         // wallFluxes' alpha |e| f on full values, written for stored ones:
         // |e| (f_s + (alpha - 1)(f_s + f_ref)) - |e| f_ref
         const C fs = (C)__ldg(k.v.st + (pp * k.v.plane + oo));
-        return ae * (fs + k.alpha[oo] * (fs + (C)k.fref[pp]));
+        return xmul(ae, xfma((C)k.alpha[oo], xadd(fs, (C)k.fref[pp]), fs));
     }
     const uint8_t edge = axis == 0 ? (NF_SOLX | NF_EDGX) : (NF_SOLY | NF_EDGY);
     if (in_box && !mirrored && !(fl & edge)) {
@@ -614,9 +630,9 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
             // alpha |e| f of wallFluxes on stored deviations (see any_node_flux)
             const C am1 = k.alpha[k.o];
             const C fv = (C)cf[0], hv = (C)ch[0];
-            const C gf = fv + am1 * (fv + (C)k.fref[i]), gh = hv + am1 * (hv + (C)k.fref[NQ + i]);
-            if (SX) { sf[k.tid] = aex * gf; sf[NT + k.tid] = aex * gh; }
-            if (SY) { sf[2 * NT + k.tid] = aey * gf; sf[3 * NT + k.tid] = aey * gh; }
+            const C gf = xfma(am1, xadd(fv, (C)k.fref[i]), fv), gh = xfma(am1, xadd(hv, (C)k.fref[NQ + i]), hv);
+            if (SX) { sf[k.tid] = xmul(aex, gf); sf[NT + k.tid] = xmul(aex, gh); }
+            if (SY) { sf[2 * NT + k.tid] = xmul(aey, gf); sf[3 * NT + k.tid] = xmul(aey, gh); }
         } else {
             if (SX) {
                 C a, b;
@@ -627,8 +643,7 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
                     a = flux_axis<S, C>(sp, k.v, k.x, k.y, i, 0, k.flag);
                     b = flux_axis<S, C>(sp, k.v, k.x, k.y, NQ + i, 0, k.flag);
                 } else {
-                    a = box_flux<S, C>(sp, cf, SX, aex);
-                    b = box_flux<S, C>(sp, ch, SX, aex);
+                    box_flux_fh<S, C, FM>(sp, cf, ch, SX, aex, a, b);
                 }
                 sf[k.tid] = a;
                 sf[NT + k.tid] = b;
@@ -642,8 +657,7 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
                     a = flux_axis<S, C>(sp, k.v, k.x, k.y, i, 1, k.flag);
                     b = flux_axis<S, C>(sp, k.v, k.x, k.y, NQ + i, 1, k.flag);
                 } else {
-                    a = box_flux<S, C>(sp, cf, SY * k.BW, aey);
-                    b = box_flux<S, C>(sp, ch, SY * k.BW, aey);
+                    box_flux_fh<S, C, FM>(sp, cf, ch, SY * k.BW, aey, a, b);
                 }
                 sf[2 * NT + k.tid] = a;
                 sf[3 * NT + k.tid] = b;
@@ -680,45 +694,60 @@ __device__ __forceinline__ void dir_fluxes(TileCtx<S, C> &k, const int i, const 
 }
 
 // divergence D = (dt/dx, dt/dy).(F_out - F_in) of cFLUX
-// (cpuLBM.cpp:1436-1470) for direction i at this node
+// (cpuLBM.cpp:1436-1470) for direction i at this node.  Every operation is
+// an explicitly rounded one, so each kernel instance (simple, wrap and
+// general tiles, any tile shape) gives a node the same bits.  FP64 keeps the
+// reference's order (each flux scaled, out and in summed, then subtracted);
+// FP32 takes the differences first (fewer operations).
 template <class S, class C, int CEX = DIR_RT, int CEY = DIR_RT>
 __device__ __forceinline__ void dir_divergence(TileCtx<S, C> &k, const int i, const C *sf, const C *ringx,
                                                const C *ringy)
 {
     const int SX = isgn(CEX != DIR_RT ? CEX : c_EX[i]), SY = isgn(CEY != DIR_RT ? CEY : c_EY[i]);
     const int NT = k.NT;
-    C of = C(0), oh = C(0), inf_ = C(0), inh = C(0);
-    bool have = false;
+    C fox = C(0), hox = C(0), fix = C(0), hix = C(0), foy = C(0), hoy = C(0), fiy = C(0), hiy = C(0);
     if (SX) {
         const int xu = k.x - SX;
         const bool inside = xu >= k.x0 && xu < k.x_end;
-        const C fi = inside ? sf[k.tid - SX] : ringx[k.ty];
-        const C hi = inside ? sf[NT + k.tid - SX] : ringx[k.TY + k.ty];
-        of = k.tdx * sf[k.tid];
-        oh = k.tdx * sf[NT + k.tid];
-        inf_ = k.tdx * fi;
-        inh = k.tdx * hi;
-        have = true;
+        fix = inside ? sf[k.tid - SX] : ringx[k.ty];
+        hix = inside ? sf[NT + k.tid - SX] : ringx[k.TY + k.ty];
+        fox = sf[k.tid];
+        hox = sf[NT + k.tid];
     }
     if (SY) {
         const int yu = k.y - SY;
         const bool inside = yu >= k.y0 && yu < k.y_end;
-        const C fi = inside ? sf[2 * NT + k.tid - SY * k.TX] : ringy[k.tx];
-        const C hi = inside ? sf[3 * NT + k.tid - SY * k.TX] : ringy[k.TX + k.tx];
-        if (have) {
-            of = of + k.tdy * sf[2 * NT + k.tid];
-            oh = oh + k.tdy * sf[3 * NT + k.tid];
-            inf_ = inf_ + k.tdy * fi;
-            inh = inh + k.tdy * hi;
+        fiy = inside ? sf[2 * NT + k.tid - SY * k.TX] : ringy[k.tx];
+        hiy = inside ? sf[3 * NT + k.tid - SY * k.TX] : ringy[k.TX + k.tx];
+        foy = sf[2 * NT + k.tid];
+        hoy = sf[3 * NT + k.tid];
+    }
+    C df, dh;
+    if constexpr (IsF32<C>::value) {
+        if (SX && SY) {
+            df = xfma(k.tdy, xsub(foy, fiy), xmul(k.tdx, xsub(fox, fix)));
+            dh = xfma(k.tdy, xsub(hoy, hiy), xmul(k.tdx, xsub(hox, hix)));
+        } else if (SX) {
+            df = xmul(k.tdx, xsub(fox, fix));
+            dh = xmul(k.tdx, xsub(hox, hix));
         } else {
-            of = k.tdy * sf[2 * NT + k.tid];
-            oh = k.tdy * sf[3 * NT + k.tid];
-            inf_ = k.tdy * fi;
-            inh = k.tdy * hi;
+            df = xmul(k.tdy, xsub(foy, fiy));
+            dh = xmul(k.tdy, xsub(hoy, hiy));
+        }
+    } else {
+        if (SX && SY) {
+            df = xsub(xadd(xmul(k.tdx, fox), xmul(k.tdy, foy)), xadd(xmul(k.tdx, fix), xmul(k.tdy, fiy)));
+            dh = xsub(xadd(xmul(k.tdx, hox), xmul(k.tdy, hoy)), xadd(xmul(k.tdx, hix), xmul(k.tdy, hiy)));
+        } else if (SX) {
+            df = xsub(xmul(k.tdx, fox), xmul(k.tdx, fix));
+            dh = xsub(xmul(k.tdx, hox), xmul(k.tdx, hix));
+        } else {
+            df = xsub(xmul(k.tdy, foy), xmul(k.tdy, fiy));
+            dh = xsub(xmul(k.tdy, hoy), xmul(k.tdy, hiy));
         }
     }
-    k.sD[i * NT + k.tid] = of - inf_;
-    k.sD[(NQ + i) * NT + k.tid] = oh - inh;
+    k.sD[i * NT + k.tid] = df;
+    k.sD[(NQ + i) * NT + k.tid] = dh;
 }
 
 // General tiles whose box crosses a periodic edge: the box cells outside
@@ -1010,8 +1039,18 @@ __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
             for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, true, G, 0, WRAPT>(k, g);
         }
     } else {
+        // general tiles: the scheme fixed at compile time for their plain
+        // nodes' faces (the boundary stencils read it at run time)
+        if (sp.fm && sizeof(S) == 4 && sp.wide) {
 #pragma unroll 1
-        for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, false, G, -1>(k, g);
+            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, false, G, 2>(k, g);
+        } else if (sp.fm) {
+#pragma unroll 1
+            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, false, G, 1>(k, g);
+        } else {
+#pragma unroll 1
+            for (int g = 0; g < GroupCfg<G>::NGROUP; ++g) dir_group<S, C, false, G, 0>(k, g);
+        }
     }
 
     // the prefetched state values: every thread waits (boundedly) for the
