@@ -197,7 +197,7 @@ typedef struct lbm_batch lbm_batch;
 
 typedef struct lbm_batch_options {
     int precision;      /* LBM_PREC_F64 / LBM_PREC_F32 */
-    int tile_x, tile_y; /* 0: chosen by the autotuner's table (16 x 16, the
+    int tile_x, tile_y; /* 0: chosen by the autotuner's table (32 x 8, the
                            shape the stencil kernels are also compiled for;
                            other shapes run the same kernels with the shape
                            read at run time, bit-identical and slower) */
@@ -278,7 +278,7 @@ typedef struct lbm_server lbm_server;
 
 typedef struct lbm_server_options {
     int precision;        /* LBM_PREC_F64 / LBM_PREC_F32, all solves */
-    int tile_x, tile_y;   /* 0: 16 x 16 */
+    int tile_x, tile_y;   /* 0: 32 x 8 */
     size_t arena_bytes;   /* device memory for resident solves; 0: hbm_fraction of the free memory */
     double hbm_fraction;  /* used when arena_bytes is 0; 0: 0.6 */
     int max_resident;     /* most solves resident at once; 0: 1024 */

@@ -26,8 +26,9 @@ def test_profile_and_launch_count(cuda_device):
     b = Batch([W.couette(nx=64, ny=48, steps=4, seed=1)], "f32")
     ms = b.profile(2)
     assert ms.shape == (6,) and (ms[:5] >= 0).all() and ms[2] > 0
-    # 4 x 3 tiles of 16 x 16: the middle row is simple (the two at the
-    # periodic x edges read the ghost columns); the rest touch the walls.
+    # 2 x 6 tiles of 32 x 8: the four middle rows are simple (the tiles at
+    # the periodic x edges read the ghost columns); the top and bottom rows
+    # touch the walls.
     # Pointwise, ghost columns of buffer 2, walls, stencil 1 (simple and
     # general kernels), walls, stencil 2 (both), + residual
     assert b.launches_per_step(False) == 8

@@ -391,9 +391,10 @@ using namespace uqlbm;
 
 struct lbm_batch {
     int prec = LBM_PREC_F64;
-    // default tile: the autotuner's pick on the 512-sample UQ ensemble, both
-    // precisions (lbm_batch_autotune re-measures for a given batch)
-    int tx = 16, ty = 16;
+    // default tile: the shape the stencil kernels are compiled for, the
+    // fastest on the 512-sample UQ ensemble (lbm_batch_autotune re-measures
+    // for a given batch)
+    int tx = TILE_CX, ty = TILE_CY;
     std::vector<uint8_t> flags_host;
     bool use_graph = true;
     int device = 0;
@@ -1301,7 +1302,7 @@ lbm_status lbm_batch_autotune(lbm_batch *b, const int *candidates, int n_candida
 {
     API_BEGIN
     if (!b) throw LbmError(LBM_ERR_INVALID, "null batch");
-    static const int defaults[] = {16, 16, 32, 8, 64, 4, 8, 32, 32, 4, 16, 8};
+    static const int defaults[] = {32, 8, 16, 16, 64, 4, 8, 32, 32, 4, 16, 8};
     if (!candidates || n_candidates <= 0) {
         candidates = defaults;
         n_candidates = 6;

@@ -941,14 +941,14 @@ size_t flux_smem_bytes_t(size_t es, int tx, int ty)
 // FLUX_WRAP is the simple code with the periodic images copied into each
 // staged box before use.  A block given a tile of another kind returns at
 // once.
-// T16: the tile shape is the default 16 x 16, compiled in (box widths,
-// strides and the thread-to-node map become constants); otherwise read from
-// the arguments.
-template <class S, class C, int MODE, int PATH, bool T16>
+// TC: the tile shape is the default TILE_CX x TILE_CY, compiled in (box
+// widths, strides and the thread-to-node map become constants); otherwise
+// read from the arguments.
+template <class S, class C, int MODE, int PATH, bool TC>
 __global__ void __launch_bounds__(256, 2) k_flux(KArgs<S> a)
 {
     extern __shared__ __align__(128) unsigned char smem_dyn[];
-    const int TX = T16 ? 16 : a.tx, TY = T16 ? 16 : a.ty, NT = TX * TY;
+    const int TX = TC ? TILE_CX : a.tx, TY = TC ? TILE_CY : a.ty, NT = TX * TY;
     const int BW = TX + 2 * HALO_X, BH = TY + 2 * HALO_Y;
     constexpr int G = FluxGroup<S>::value;
     constexpr int NST = GroupCfg<G>::NSTAGE;
@@ -1473,22 +1473,22 @@ template cudaError_t launch_set_macro<float>(const SampleParams *, int, float *,
 // phase: 0 pointwise stages, 1 stencil phase over buffer 2, 2 RK3 final
 // stencil phase over buffer 3, 3/4 wall fluxes of buffer 2/3.  rk selects
 // the method of the tiles passed (one method per launch).
-template <class S, class C, int PATH, bool T16>
+template <class S, class C, int PATH, bool TC>
 void launch_flux_t(int mode, const KArgs<S> &k, int ntiles, int NT, size_t sm, cudaStream_t st)
 {
     switch (mode) {
-    case 1: k_flux<S, C, 1, PATH, T16><<<ntiles, NT, sm, st>>>(k); break;
-    case 2: k_flux<S, C, 2, PATH, T16><<<ntiles, NT, sm, st>>>(k); break;
-    case 3: k_flux<S, C, 3, PATH, T16><<<ntiles, NT, sm, st>>>(k); break;
-    case 4: k_flux<S, C, 4, PATH, T16><<<ntiles, NT, sm, st>>>(k); break;
-    default: k_flux<S, C, 5, PATH, T16><<<ntiles, NT, sm, st>>>(k); break;
+    case 1: k_flux<S, C, 1, PATH, TC><<<ntiles, NT, sm, st>>>(k); break;
+    case 2: k_flux<S, C, 2, PATH, TC><<<ntiles, NT, sm, st>>>(k); break;
+    case 3: k_flux<S, C, 3, PATH, TC><<<ntiles, NT, sm, st>>>(k); break;
+    case 4: k_flux<S, C, 4, PATH, TC><<<ntiles, NT, sm, st>>>(k); break;
+    default: k_flux<S, C, 5, PATH, TC><<<ntiles, NT, sm, st>>>(k); break;
     }
 }
 
 template <class S, class C, int PATH>
 void launch_flux(int mode, const KArgs<S> &k, int ntiles, int NT, size_t sm, cudaStream_t st)
 {
-    if (k.tx == 16 && k.ty == 16) launch_flux_t<S, C, PATH, true>(mode, k, ntiles, NT, sm, st);
+    if (k.tx == TILE_CX && k.ty == TILE_CY) launch_flux_t<S, C, PATH, true>(mode, k, ntiles, NT, sm, st);
     else launch_flux_t<S, C, PATH, false>(mode, k, ntiles, NT, sm, st);
 }
 

@@ -21,6 +21,12 @@ constexpr int STATUS_TIMEOUT = 4;    // a bounded device-side wait ran out
 // 13 planes (the f or the h half of the state, prefetched for the update)
 constexpr int MAPS_PER_SAMPLE = 3;
 constexpr int PREFETCH_PLANES = 13;
+// the default tile shape, also compiled into the stencil kernels (box
+// widths, strides and the thread-to-node map become constants); other shapes
+// run the same kernels with the shape read at run time.  A tile row of 32 is
+// one warp: a row's x neighbours sit in the same warp and its staged-box
+// reads are unit-stride across the warp.
+constexpr int TILE_CX = 32, TILE_CY = 8;
 
 struct WallNode {
     int sample, x, y, pad;

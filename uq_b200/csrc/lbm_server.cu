@@ -129,7 +129,7 @@ using namespace uqlbm;
 
 struct lbm_server {
     int prec = LBM_PREC_F32;
-    int tx = 16, ty = 16;
+    int tx = TILE_CX, ty = TILE_CY;
     int device = 0;
     bool use_graph = true;
     int max_resident = 1024, max_queued = 0, poll_steps = 32;

@@ -372,7 +372,7 @@ class Batch:
         """Pick the fastest tile shape for this batch (state unchanged);
         returns ((tile_x, tile_y), {candidate: ms per step})."""
         if candidates is None:
-            candidates = [(16, 16), (32, 8), (64, 4), (8, 32), (32, 4), (16, 8)]
+            candidates = [(32, 8), (16, 16), (64, 4), (8, 32), (32, 4), (16, 8)]
         flat = np.array([v for c in candidates for v in c], dtype=np.int32)
         chosen = np.zeros(2, dtype=np.int32)
         ms = np.zeros(len(candidates))
